@@ -1,0 +1,21 @@
+"""galoisgpu_b200 -- B200 (sm_100a) frontier-traversal engine for the
+data-driven worklist BFS and SSSP path of LonestarGPU v3.
+
+The compute lives in libgft.so (hand-written CUDA for sm_100a behind the C
+ABI of include/gft.h); this package is the Python host side.
+"""
+
+from .graph import (  # noqa: F401
+    DEFAULT_DELTA,
+    GFT_NO_PARENT,
+    INF,
+    CSRGraph,
+    DeviceGraph,
+    Engine,
+    Tune,
+    output,
+    reach_stats,
+)
+from ._lib import GftError, load  # noqa: F401
+
+__version__ = "0.1.0"

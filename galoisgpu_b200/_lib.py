@@ -1,0 +1,161 @@
+"""ctypes binding of libgft.so (the C ABI declared in include/gft.h).
+
+The library is built in-tree (``python -m galoisgpu_b200.build``).  Loading
+fails loudly when it is missing: there is no Python or CPU fallback for any
+traversal.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import threading
+from pathlib import Path
+
+LIB_PATH = Path(__file__).resolve().with_name("libgft.so")
+
+GFT_INF = 0x7FFFFFFF
+GFT_NO_PARENT = 0xFFFFFFFF
+
+STATUS_NAMES = {
+    0: "GFT_OK",
+    1: "GFT_ERR_INVALID_ARG",
+    2: "GFT_ERR_IO",
+    3: "GFT_ERR_FORMAT",
+    4: "GFT_ERR_CUDA",
+    5: "GFT_ERR_OOM",
+    6: "GFT_ERR_TIMEOUT",
+    7: "GFT_ERR_OVERFLOW",
+    8: "GFT_ERR_NOT_SUPPORTED",
+    9: "GFT_ERR_BUSY",
+}
+
+
+class GftError(RuntimeError):
+    """A libgft call returned a non-zero gft_status."""
+
+    def __init__(self, status: int, message: str):
+        self.status = status
+        self.status_name = STATUS_NAMES.get(status, f"status {status}")
+        super().__init__(f"{self.status_name}: {message}")
+
+
+class Csr(C.Structure):
+    _fields_ = [
+        ("nnodes", C.c_uint32),
+        ("nedges", C.c_uint32),
+        ("row_start", C.POINTER(C.c_uint32)),
+        ("edge_dst", C.POINTER(C.c_uint32)),
+        ("edge_data", C.POINTER(C.c_int32)),
+    ]
+
+
+class Stats(C.Structure):
+    _fields_ = [
+        ("levels", C.c_uint32),
+        ("iterations", C.c_uint32),
+        ("vertices_reached", C.c_uint64),
+        ("edges_scanned", C.c_uint64),
+        ("pushes", C.c_uint64),
+        ("kernel_ms", C.c_float),
+        ("grid_blocks", C.c_uint32),
+        ("block_threads", C.c_uint32),
+    ]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+class Tuning(C.Structure):
+    _fields_ = [
+        ("block_threads", C.c_uint32),
+        ("blocks_per_sm", C.c_uint32),
+        ("hub_degree", C.c_uint32),
+        ("timeout_ms", C.c_uint32),
+        ("test_skip_block", C.c_int32),
+    ]
+
+
+class GenParams(C.Structure):
+    _fields_ = [
+        ("kind", C.c_uint32),
+        ("rows", C.c_uint32),
+        ("cols", C.c_uint32),
+        ("scale", C.c_uint32),
+        ("edge_factor", C.c_uint32),
+        ("a_q32", C.c_uint32),
+        ("b_q32", C.c_uint32),
+        ("c_q32", C.c_uint32),
+        ("delete_ppm", C.c_uint32),
+        ("shortcut_ppm", C.c_uint32),
+        ("max_weight", C.c_uint32),
+        ("seed", C.c_uint64),
+    ]
+
+
+# name -> (restype, argtypes); every symbol include/gft.h declares.
+_P = C.c_void_p
+_SIGS: dict[str, tuple] = {
+    "gft_version": (C.c_int, []),
+    "gft_last_error": (C.c_char_p, []),
+    "gft_status_string": (C.c_char_p, [C.c_int]),
+    "gft_gr_read": (C.c_int, [C.c_char_p, C.POINTER(Csr)]),
+    "gft_gr_write": (C.c_int, [C.c_char_p, C.POINTER(Csr)]),
+    "gft_csr_free": (None, [C.POINTER(Csr)]),
+    "gft_gen_grid": (C.c_int, [C.c_uint32, C.c_uint32, C.c_uint64, C.c_uint32, C.POINTER(Csr)]),
+    "gft_gen_road": (C.c_int, [C.c_uint32, C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32, C.POINTER(Csr)]),
+    "gft_gen_rmat": (
+        C.c_int,
+        [C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint64, C.c_uint32, C.POINTER(Csr)],
+    ),
+    "gft_pick_sources": (C.c_int, [C.POINTER(Csr), C.c_uint64, C.c_uint32, C.POINTER(C.c_uint32)]),
+    "gft_graph_upload": (C.c_int, [C.c_int, C.POINTER(Csr), _P, C.POINTER(_P)]),
+    "gft_graph_wrap": (C.c_int, [C.c_int, C.c_uint32, C.c_uint32, _P, _P, _P, C.POINTER(_P)]),
+    "gft_graph_generate": (C.c_int, [C.c_int, C.POINTER(GenParams), _P, C.POINTER(_P)]),
+    "gft_graph_info": (C.c_int, [_P, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.POINTER(C.c_int)]),
+    "gft_graph_arrays": (C.c_int, [_P, C.POINTER(_P), C.POINTER(_P), C.POINTER(_P)]),
+    "gft_graph_download": (C.c_int, [_P, C.POINTER(Csr)]),
+    "gft_graph_free": (None, [_P]),
+    "gft_engine_create": (C.c_int, [C.c_int, C.POINTER(_P)]),
+    "gft_engine_destroy": (None, [_P]),
+    "gft_engine_scratch_bytes": (C.c_size_t, [_P]),
+    "gft_bfs": (C.c_int, [_P, _P, C.c_uint32, _P, _P, C.POINTER(Tuning), _P, C.POINTER(Stats)]),
+    "gft_sssp": (C.c_int, [_P, _P, C.c_uint32, C.c_int32, _P, _P, C.POINTER(Tuning), _P, C.POINTER(Stats)]),
+    "gft_bfs_host": (C.c_int, [_P, _P, C.c_uint32, _P, _P, C.POINTER(Tuning), _P, C.POINTER(Stats)]),
+    "gft_sssp_host": (C.c_int, [_P, _P, C.c_uint32, C.c_int32, _P, _P, C.POINTER(Tuning), _P, C.POINTER(Stats)]),
+    "gft_reach_stats": (C.c_int, [_P, _P, _P, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
+    "gft_write_output": (C.c_int, [C.c_char_p, C.c_uint32, _P]),
+}
+
+_lock = threading.Lock()
+_lib: C.CDLL | None = None
+
+
+def load() -> C.CDLL:
+    """Loads libgft.so (once) and declares every exported signature."""
+    global _lib
+    with _lock:
+        if _lib is not None:
+            return _lib
+        if not LIB_PATH.exists():
+            raise ImportError(
+                f"{LIB_PATH} is not built; run `python -m galoisgpu_b200.build` "
+                "(there is no fallback implementation)"
+            )
+        lib = C.CDLL(str(LIB_PATH))
+        for name, (res, args) in _SIGS.items():
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = lib
+        return lib
+
+
+def declared_symbols() -> list[str]:
+    return list(_SIGS)
+
+
+def check(status: int) -> None:
+    """Raises GftError for a non-zero status, with the library's message."""
+    if status != 0:
+        msg = load().gft_last_error()
+        raise GftError(status, msg.decode() if msg else "")

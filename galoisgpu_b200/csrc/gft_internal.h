@@ -1,0 +1,122 @@
+// gft_internal.h -- shared definitions of the libgft implementation files.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stdio.h>
+
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "gft.h"
+
+namespace gft {
+
+// Thread-local message of the last failure (gft_last_error).
+void set_error(const char *fmt, ...);
+void clear_error();
+
+// Returns `s` after recording a formatted message.
+gft_status fail(gft_status s, const char *fmt, ...);
+
+#define GFT_CUDA_TRY(call)                                                                             \
+    do {                                                                                               \
+        cudaError_t e_ = (call);                                                                       \
+        if (e_ != cudaSuccess)                                                                         \
+            return ::gft::fail(e_ == cudaErrorMemoryAllocation ? GFT_ERR_OOM : GFT_ERR_CUDA,           \
+                               "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__,       \
+                               __LINE__);                                                              \
+    } while (0)
+
+#define GFT_TRY(call)                        \
+    do {                                     \
+        gft_status s_ = (call);              \
+        if (s_ != GFT_OK) return s_;         \
+    } while (0)
+
+// Device-resident graph.  The arrays are owned unless `wrapped`.
+struct DeviceGraph {
+    int device = 0;
+    uint32_t nnodes = 0, nedges = 0;
+    uint32_t *row_start = nullptr;
+    uint32_t *edge_dst = nullptr;
+    int32_t *edge_data = nullptr;
+    bool wrapped = false;
+};
+
+// Lazily grown device allocation owned by an engine.
+struct Scratch {
+    void *ptr = nullptr;
+    size_t bytes = 0;
+    gft_status ensure(size_t want);
+    void release();
+};
+
+// Control block of one persistent traversal, zeroed before every launch.
+// Counters are triple buffered by iteration (slot = iteration % 3): a slot is
+// read during its own iteration, written by the iteration before it and
+// cleared by the iteration after it, so no extra grid barrier is needed to
+// recycle them.
+// Every counter that is hit by atomics sits alone in a 128-byte line.
+struct alignas(128) CtlLine {
+    unsigned long long v;
+    unsigned long long pad[15];
+};
+
+struct TraversalCtl {
+    CtlLine barrier;       // grid barrier arrival counter (u64)
+    CtlLine qlen[3];       // frontier (SSSP: near pile) length per iteration slot (u32)
+    CtlLine claim[3];      // work-claim cursor per iteration slot (u32)
+    CtlLine hub[3];        // (hubs << 32) | hub chunks per iteration slot (u64)
+    CtlLine hub_claim[3];  // hub chunk cursor per iteration slot (u32)
+    CtlLine far_len[3];    // SSSP far pile length per phase slot (u32)
+    CtlLine far_min[3];    // SSSP least distance sent to the far pile per phase slot (u32)
+    // Cold fields, written once per launch.
+    unsigned error;        // gft_status recorded by the device (0 = none)
+    unsigned error_where;  // barrier episode or queue index of the failure
+    unsigned levels;       // BFS levels / SSSP phases
+    unsigned iterations;   // grid-synchronous iterations
+    unsigned threshold;    // SSSP final bucket threshold
+    unsigned pad0;
+    unsigned long long edges;    // edges scanned
+    unsigned long long pushes;   // frontier pushes
+    unsigned long long reached;  // vertices reached (BFS)
+};
+
+__host__ __device__ inline unsigned *u32_of(CtlLine &l) { return reinterpret_cast<unsigned *>(&l.v); }
+
+struct LaunchShape {
+    int block_threads = 512;
+    int blocks = 0;
+    int blocks_per_sm = 0;
+    int sms = 0;
+};
+
+}  // namespace gft
+
+struct gft_graph {
+    gft::DeviceGraph g;
+};
+
+struct gft_engine {
+    int device = 0;
+    int sms = 0;
+    int cc_major = 0, cc_minor = 0;
+    gft::Scratch scratch;    // traversal state (queues, bitmaps, stamps)
+    gft::Scratch ctl;        // TraversalCtl
+    gft::Scratch aux;        // per-call small buffers (e.g. the source id)
+    void *host_ctl = nullptr;  // pinned copy of the TraversalCtl read back after a launch
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    std::mutex mu;
+};
+
+namespace gft {
+// Resolves tuning defaults and the cooperative grid for a kernel.
+gft_status resolve_shape(gft_engine *e, const void *kernel, int block_threads, int blocks_per_sm,
+                         size_t dyn_smem, LaunchShape *out);
+gft_status check_engine_graph(gft_engine *e, const gft_graph *g);
+// Runs one BFS (is_sssp false) or SSSP query; caller holds e->mu.
+gft_status run_traversal(bool is_sssp, gft_engine *e, const gft_graph *g, uint32_t src, int32_t delta, int32_t *d_out,
+                         uint32_t *d_parent, const gft_tuning *tune, cudaStream_t stream, gft_stats *stats);
+gft_status reach_stats(const gft_graph *g, const int32_t *d_val, cudaStream_t stream, uint64_t *v_r, uint64_t *e_r);
+}  // namespace gft

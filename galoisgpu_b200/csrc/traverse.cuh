@@ -1,0 +1,222 @@
+// traverse.cuh -- device building blocks of the persistent traversal kernels.
+//
+//   GridSync      bounded-wait grid barrier for a cooperative (co-resident)
+//                 launch; replaces GlobalBarrier (rt/include/gbar.cuh:75-121),
+//                 whose wait has no limit.
+//   WarpQueue     warp-aggregated frontier append: ballot + popc + lane-mask
+//                 prefix into a per-warp shared-memory buffer, flushed 32
+//                 items at a time with one atomicAdd and one 128-byte store;
+//                 replaces Worklist2::setup_push_warp_one / do_push
+//                 (rt/include/worklist.h:349-368,415-420), which spends one
+//                 global atomic per warp per visit round.
+//   warp_flatten  expands the edges of up to 32 small-degree vertices (one
+//                 per lane) as one flattened, load-balanced edge list: a
+//                 shuffle-based prefix sum of the degrees and a 5-step
+//                 shuffle binary search gives every lane its edge; replaces
+//                 the CTA-wide cub::BlockScan edge batches of the reference's
+//                 fine-grained tier (apps/bfs/kernel.cu:246-272,
+//                 rt/include/internal.h:60-158).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "gft_internal.h"
+
+namespace gft {
+namespace dev {
+
+constexpr unsigned kFull = 0xFFFFFFFFu;
+
+__device__ __forceinline__ unsigned long long globaltimer_ns()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+__device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long *p)
+{
+    unsigned long long v;
+    asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ unsigned ld_relaxed_u32(const unsigned *p)
+{
+    unsigned v;
+    asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ unsigned long long ld_relaxed_u64(const unsigned long long *p)
+{
+    unsigned long long v;
+    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ void red_release_add_u64(unsigned long long *p, unsigned long long v)
+{
+    asm volatile("red.release.gpu.global.add.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+__device__ __forceinline__ unsigned lanemask_lt()
+{
+    unsigned m;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+    return m;
+}
+
+// Records the first device-side failure; later ones keep the first code.
+__device__ __forceinline__ void raise_error(unsigned *err, unsigned *where, unsigned code, unsigned site)
+{
+    if (atomicCAS(err, 0u, code) == 0u) atomicExch(where, site);
+}
+
+// Grid barrier over a cooperative launch.  Arrivals count up on one 64-bit
+// counter; episode k is complete when the counter reaches k * nblocks, so the
+// counter never needs resetting inside the launch.  Thread 0 of each CTA
+// waits with a bounded spin (globaltimer); on expiry it records
+// GFT_ERR_TIMEOUT, and every waiter also leaves as soon as any CTA has
+// recorded an error, so no CTA can be left spinning.
+struct GridSync {
+    unsigned long long *counter;
+    unsigned *error;
+    unsigned *error_where;
+    unsigned nblocks;
+    unsigned epoch;
+    unsigned long long timeout_ns;
+
+    // Returns false when the traversal must stop.
+    __device__ __forceinline__ bool sync()
+    {
+        __shared__ unsigned s_err;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            epoch++;
+            unsigned long long target = (unsigned long long)epoch * nblocks;
+            __threadfence();
+            red_release_add_u64(counter, 1ull);
+            unsigned long long t0 = 0;
+            unsigned spins = 0;
+            while (ld_acquire_u64(counter) < target) {
+                if (ld_relaxed_u32(error)) break;
+                if ((++spins & 127u) == 0) {
+                    unsigned long long now = globaltimer_ns();
+                    if (t0 == 0) t0 = now;
+                    else if (now - t0 > timeout_ns) {
+                        raise_error(error, error_where, GFT_ERR_TIMEOUT, epoch);
+                        break;
+                    }
+                }
+            }
+            __threadfence();
+            s_err = ld_relaxed_u32(error);
+        }
+        __syncthreads();
+        return s_err == 0;
+    }
+};
+
+// Warp-aggregated append to a global queue through a 64-entry per-warp
+// shared-memory buffer.  `count` is warp uniform.  All 32 lanes must call
+// push() and flush() together.
+struct WarpQueue {
+    uint32_t *buf;       // this warp's 64 shared-memory slots
+    unsigned count;
+    uint32_t *queue;     // global destination
+    unsigned *len;       // global length counter
+    unsigned cap;        // capacity of `queue`
+    unsigned *err, *err_where;
+
+    __device__ __forceinline__ void store32(unsigned lane, unsigned n)
+    {
+        unsigned base = 0;
+        if (lane == 0) base = atomicAdd(len, n);
+        base = __shfl_sync(kFull, base, 0);
+        if (base + n > cap) {
+            if (lane == 0) raise_error(err, err_where, GFT_ERR_OVERFLOW, base);
+        } else if (lane < n) {
+            queue[base + lane] = buf[lane];
+        }
+    }
+
+    __device__ __forceinline__ void push(bool p, uint32_t item, unsigned lane)
+    {
+        unsigned mask = __ballot_sync(kFull, p);
+        if (mask == 0) return;
+        if (p) buf[count + __popc(mask & lanemask_lt())] = item;
+        count += __popc(mask);
+        if (count >= 32) {
+            __syncwarp();
+            store32(lane, 32);
+            unsigned rest = count - 32;
+            uint32_t x = lane < rest ? buf[32 + lane] : 0u;
+            __syncwarp();
+            if (lane < rest) buf[lane] = x;
+            __syncwarp();
+            count = rest;
+        }
+    }
+
+    __device__ __forceinline__ void flush(unsigned lane)
+    {
+        if (count == 0) return;
+        __syncwarp();
+        store32(lane, count);
+        __syncwarp();
+        count = 0;
+    }
+};
+
+// Inclusive warp prefix sum.
+__device__ __forceinline__ uint32_t warp_incl_sum(uint32_t x, unsigned lane)
+{
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        uint32_t t = __shfl_up_sync(kFull, x, o);
+        if (lane >= (unsigned)o) x += t;
+    }
+    return x;
+}
+
+// Flattened expansion of the edge ranges [start, start+deg) held one per
+// lane.  For each batch of 32 edges, calls f(valid, owner_lane, edge) on all
+// lanes; the owner is the lane whose range holds the edge.
+template <typename F>
+__device__ __forceinline__ void warp_flatten(uint32_t start, uint32_t deg, unsigned lane, F &&f)
+{
+    uint32_t incl = warp_incl_sum(deg, lane);
+    uint32_t total = __shfl_sync(kFull, incl, 31);
+    uint32_t excl = incl - deg;
+    for (uint32_t base = 0; base < total; base += 32) {
+        uint32_t g = base + lane;
+        int j = 0;
+#pragma unroll
+        for (int step = 16; step >= 1; step >>= 1) {
+            uint32_t ex = __shfl_sync(kFull, excl, j + step);
+            if (ex <= g) j += step;
+        }
+        uint32_t ostart = __shfl_sync(kFull, start, j);
+        uint32_t oexcl = __shfl_sync(kFull, excl, j);
+        f(g < total, j, ostart + (g - oexcl));
+    }
+}
+
+// Block-wide sum of a 64-bit value into *dst (one atomic per warp).
+__device__ __forceinline__ void warp_add_u64(unsigned long long *dst, unsigned long long v, unsigned lane)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(kFull, v, o);
+    if (lane == 0 && v) atomicAdd(dst, v);
+}
+
+__device__ __forceinline__ unsigned warp_min_u32(unsigned v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = min(v, __shfl_xor_sync(kFull, v, o));
+    return v;
+}
+
+}  // namespace dev
+}  // namespace gft

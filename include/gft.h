@@ -1,0 +1,223 @@
+/*
+ * gft.h -- C ABI of the B200 frontier-traversal engine (libgft.so).
+ *
+ * The engine replaces the data-driven worklist BFS and SSSP of LonestarGPU
+ * v3 (apps/bfs, apps/sssp).  Every entry point below names the reference
+ * interface it stands in for (file:line within the reference project).
+ *
+ * Conventions
+ *   - Plain C types only: pointers, sizes, integers.  No exceptions cross
+ *     this boundary and nothing calls exit(): every function returns a
+ *     gft_status (0 = GFT_OK); gft_last_error() gives a message for the
+ *     calling thread's last failure.
+ *   - Vertex and edge ids are uint32 (the reference's index_type,
+ *     rt/include/csr_graph.h:22); levels and distances are int32 with
+ *     GFT_INF = INT_MAX for unreached vertices (apps/bfs/kernel.cu:16).
+ *   - Output buffers are caller-owned.  Functions that take "d_" pointers
+ *     want device memory; "h_" pointers are host memory (pinned host memory
+ *     gives the fastest copies).
+ *   - Work is enqueued on the caller's stream (NULL = legacy default
+ *     stream).  Passing a gft_stats* makes the call wait for the stream and
+ *     fill the statistics; passing NULL keeps the call asynchronous.
+ *   - A gft_engine owns the traversal scratch (frontier queues, visited
+ *     bitmaps, counters) for one device; calls on one engine must not
+ *     overlap in time.  Use one engine per host thread / stream for
+ *     concurrency.
+ */
+#ifndef GFT_H
+#define GFT_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define GFT_API __attribute__((visibility("default")))
+#else
+#define GFT_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GFT_VERSION 1
+#define GFT_INF 0x7FFFFFFF
+#define GFT_NO_PARENT 0xFFFFFFFFu
+
+typedef enum gft_status {
+    GFT_OK = 0,
+    GFT_ERR_INVALID_ARG = 1,   /* bad pointer, size or option                     */
+    GFT_ERR_IO = 2,            /* open/read/write failed                          */
+    GFT_ERR_FORMAT = 3,        /* malformed .gr file                              */
+    GFT_ERR_CUDA = 4,          /* a CUDA runtime call failed                      */
+    GFT_ERR_OOM = 5,           /* device or host allocation failed / over budget  */
+    GFT_ERR_TIMEOUT = 6,       /* a bounded device-side wait expired              */
+    GFT_ERR_OVERFLOW = 7,      /* a queue capacity or distance range was exceeded */
+    GFT_ERR_NOT_SUPPORTED = 8, /* device is not sm_100 or feature unavailable     */
+    GFT_ERR_BUSY = 9           /* serving queue full                              */
+} gft_status;
+
+/* Host CSR graph; field meaning as CSRGraph (rt/include/csr_graph.h:96-100). */
+typedef struct gft_csr {
+    uint32_t nnodes;
+    uint32_t nedges;
+    uint32_t *row_start; /* nnodes + 1 entries, row_start[nnodes] == nedges */
+    uint32_t *edge_dst;  /* nedges entries                                  */
+    int32_t *edge_data;  /* nedges entries, or NULL for an unweighted graph  */
+} gft_csr;
+
+typedef struct gft_graph gft_graph;   /* device-resident graph            */
+typedef struct gft_engine gft_engine; /* per-device traversal scratch     */
+
+typedef struct gft_stats {
+    uint32_t levels;            /* BFS: number of levels (max level + 1); SSSP: phases */
+    uint32_t iterations;        /* grid-synchronous iterations run                     */
+    uint64_t vertices_reached;  /* V_r                                                 */
+    uint64_t edges_scanned;     /* edges read by the traversal (with re-relaxations)   */
+    uint64_t pushes;            /* frontier pushes                                     */
+    float kernel_ms;            /* device time of the traversal launch                 */
+    uint32_t grid_blocks;       /* persistent grid size used                           */
+    uint32_t block_threads;
+} gft_stats;
+
+/* Tunables of one traversal; zero fields take the engine defaults. */
+typedef struct gft_tuning {
+    uint32_t block_threads;   /* 256, 512 or 1024                                   */
+    uint32_t blocks_per_sm;   /* persistent CTAs per SM (capped by occupancy)       */
+    uint32_t hub_degree;      /* degree at which a vertex is split across the grid  */
+    uint32_t timeout_ms;      /* bound on every device-side wait                    */
+    int32_t test_skip_block;  /* test hook: CTA that never arrives (-1 = none)      */
+} gft_tuning;
+
+/* ---------------------------------------------------------------------------
+ * Library
+ * ------------------------------------------------------------------------- */
+GFT_API int gft_version(void);
+/* Message of the calling thread's last failed call ("" if none). */
+GFT_API const char *gft_last_error(void);
+GFT_API const char *gft_status_string(gft_status s);
+
+/* ---------------------------------------------------------------------------
+ * .gr binary CSR files.
+ * gft_gr_read replaces CSRGraph::read / readFromGR
+ * (rt/src/csr_graph.cu:152-241).  Layout (little endian): u64 version (=1),
+ * u64 sizeEdgeTy (0 or 4), u64 numNodes, u64 numEdges, u64 outIdx[numNodes]
+ * (end offsets), u32 outs[numEdges], u32 pad if numEdges is odd, u32
+ * edgeData[numEdges] if sizeEdgeTy != 0.  Unlike the reference (which only
+ * prints a warning, csr_graph.cu:219), an edge whose destination is
+ * >= numNodes, a non-monotone outIdx or a truncated file is rejected with
+ * GFT_ERR_FORMAT.  Arrays are malloc'd; release with gft_csr_free.
+ * ------------------------------------------------------------------------- */
+GFT_API gft_status gft_gr_read(const char *path, gft_csr *out);
+GFT_API gft_status gft_gr_write(const char *path, const gft_csr *g);
+GFT_API void gft_csr_free(gft_csr *g);
+
+/* ---------------------------------------------------------------------------
+ * Seeded synthetic graphs (host side).  Deterministic functions of their
+ * arguments; the same graph is produced by the device generators.
+ *   grid:  r x c 4-neighbour grid, ids r*cols+c, both directions; weights
+ *          1 when unit_weights, else uniform [1, max_weight] per undirected
+ *          edge.
+ *   road:  side x side grid with each undirected edge deleted with
+ *          probability delete_ppm/1e6, plus shortcut_ppm/1e6 * (grid edges)
+ *          random undirected shortcuts; weights uniform [1, max_weight].
+ *   rmat:  2^scale vertices, edge_factor * 2^scale samples with quadrant
+ *          probabilities a,b,c (d = 1-a-b-c) in parts per 2^32, seeded
+ *          vertex permutation, symmetrised, self loops and duplicates
+ *          removed; weights uniform [1, max_weight] when max_weight > 0.
+ * All graphs are symmetric with rows sorted by destination.
+ * ------------------------------------------------------------------------- */
+GFT_API gft_status gft_gen_grid(uint32_t rows, uint32_t cols, uint64_t seed, uint32_t max_weight, gft_csr *out);
+GFT_API gft_status gft_gen_road(uint32_t side, uint64_t seed, uint32_t delete_ppm, uint32_t shortcut_ppm,
+                        uint32_t max_weight, gft_csr *out);
+GFT_API gft_status gft_gen_rmat(uint32_t scale, uint32_t edge_factor, uint32_t a_q32, uint32_t b_q32, uint32_t c_q32,
+                        uint64_t seed, uint32_t max_weight, gft_csr *out);
+/* Draws k distinct sources with out-degree > 0 (k <= nnodes) from seed. */
+GFT_API gft_status gft_pick_sources(const gft_csr *g, uint64_t seed, uint32_t k, uint32_t *out_sources);
+
+/* ---------------------------------------------------------------------------
+ * Device graphs.
+ * gft_graph_upload replaces CSRGraph::copy_to_gpu (rt/src/csr_graph.cu:250-261):
+ * it allocates device arrays and copies row_start, edge_dst and edge_data
+ * (edge_data only when present) on `stream`, then waits for the copies.
+ * gft_graph_wrap adopts caller-owned device arrays without copying; the
+ * caller keeps them alive until gft_graph_free.
+ * ------------------------------------------------------------------------- */
+GFT_API gft_status gft_graph_upload(int device, const gft_csr *g, void *stream, gft_graph **out);
+GFT_API gft_status gft_graph_wrap(int device, uint32_t nnodes, uint32_t nedges, const uint32_t *d_row_start,
+                          const uint32_t *d_edge_dst, const int32_t *d_edge_data, gft_graph **out);
+/* Generates a synthetic graph directly in device memory (same result as the
+ * host generators above; kind 0 = grid, 1 = road, 2 = rmat, with the
+ * parameters of those functions in p[0..7] as listed in gft_gen_params). */
+typedef struct gft_gen_params {
+    uint32_t kind;          /* 0 grid, 1 road, 2 rmat                        */
+    uint32_t rows, cols;    /* grid; road uses rows as the side              */
+    uint32_t scale, edge_factor, a_q32, b_q32, c_q32; /* rmat              */
+    uint32_t delete_ppm, shortcut_ppm;                  /* road              */
+    uint32_t max_weight;    /* 0 = unweighted (grid: 1 = unit weights)       */
+    uint64_t seed;
+} gft_gen_params;
+GFT_API gft_status gft_graph_generate(int device, const gft_gen_params *p, void *stream, gft_graph **out);
+GFT_API gft_status gft_graph_info(const gft_graph *g, uint32_t *nnodes, uint32_t *nedges, int *weighted);
+/* Device pointers of a graph (any may be NULL). */
+GFT_API gft_status gft_graph_arrays(const gft_graph *g, const uint32_t **d_row_start, const uint32_t **d_edge_dst,
+                            const int32_t **d_edge_data);
+/* Copies a device graph back to a host CSR (arrays malloc'd). */
+GFT_API gft_status gft_graph_download(const gft_graph *g, gft_csr *out);
+GFT_API void gft_graph_free(gft_graph *g);
+
+/* ---------------------------------------------------------------------------
+ * Engines
+ * ------------------------------------------------------------------------- */
+GFT_API gft_status gft_engine_create(int device, gft_engine **out);
+GFT_API void gft_engine_destroy(gft_engine *e);
+/* Bytes of device scratch the engine currently holds. */
+GFT_API size_t gft_engine_scratch_bytes(const gft_engine *e);
+
+/* ---------------------------------------------------------------------------
+ * Single queries.
+ *
+ * gft_bfs replaces gg_main of apps/bfs (apps/bfs/kernel.cu:380-393) with its
+ * persistent driver gg_main_pipe_1_gpu_gb (:312-334): d_level[v] = hop
+ * distance from src, GFT_INF if unreached.  If d_parent is non-NULL it
+ * receives a BFS tree: parent[src] = src, parent[v] = a vertex p with an
+ * edge (p, v) and level[p] + 1 == level[v], GFT_NO_PARENT if unreached.
+ *
+ * gft_sssp replaces gg_main of apps/sssp (apps/sssp/kernel.cu:455-480) with
+ * gg_main_pipe_1_gpu_gb (:355-391): d_dist[v] = shortest-path distance from
+ * src under int32 edge weights (reference -d delta: `delta` is the bucket
+ * width, > 0, and affects only the schedule), GFT_INF if unreached.  An
+ * unweighted graph has weight 0 on every edge, as in the reference (whose
+ * edge_data is calloc'd, rt/src/csr_graph.cu:211).  d_parent as for BFS with
+ * dist[p] + w(p, v) == dist[v] (weights must be >= 1 for a tree).
+ * Returns GFT_ERR_OVERFLOW if a distance would exceed INT_MAX - 1.
+ * ------------------------------------------------------------------------- */
+GFT_API gft_status gft_bfs(gft_engine *e, const gft_graph *g, uint32_t src, int32_t *d_level, uint32_t *d_parent,
+                   const gft_tuning *tune, void *stream, gft_stats *stats);
+GFT_API gft_status gft_sssp(gft_engine *e, const gft_graph *g, uint32_t src, int32_t delta, int32_t *d_dist,
+                    uint32_t *d_parent, const gft_tuning *tune, void *stream, gft_stats *stats);
+
+/* Host-buffer variants (the end-to-end path of the reference's skel driver,
+ * skelapp/skel.cu:159-174: traversal, then copy of node_data to the host).
+ * The source goes to the device and the nnodes results come back inside the
+ * call; h_out (and h_parent if non-NULL) are host arrays of nnodes entries.
+ * The call returns when the results are in host memory. */
+GFT_API gft_status gft_bfs_host(gft_engine *e, const gft_graph *g, uint32_t src, int32_t *h_level, uint32_t *h_parent,
+                        const gft_tuning *tune, void *stream, gft_stats *stats);
+GFT_API gft_status gft_sssp_host(gft_engine *e, const gft_graph *g, uint32_t src, int32_t delta, int32_t *h_dist,
+                         uint32_t *h_parent, const gft_tuning *tune, void *stream, gft_stats *stats);
+
+/* Reach statistics of a result already on the device: V_r (vertices with a
+ * finite value) and E_r (sum of their out-degrees, the edges a top-down
+ * traversal must scan).  Waits for `stream`. */
+GFT_API gft_status gft_reach_stats(const gft_graph *g, const int32_t *d_val, void *stream, uint64_t *v_r, uint64_t *e_r);
+
+/* Writes values in the reference's output format, "%d %d\n" or "%d INF\n"
+ * per node (apps/bfs/support.cu:27-45, apps/sssp/support.cu:34-53).
+ * path "-" writes to stdout. */
+GFT_API gft_status gft_write_output(const char *path, uint32_t nnodes, const int32_t *h_val);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GFT_H */

@@ -1,0 +1,138 @@
+"""ctypes binding of the CPU oracle (oracle/oracle.c -> oracle/liboracle.so).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, by __graft_entry__.smoke() as
+the checker and by bench.py's CPU-baseline leg.  The galoisgpu_b200 package
+never imports it.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB = HERE / "liboracle.so"
+INF = 0x7FFFFFFF
+NO_PARENT = 0xFFFFFFFF
+
+_lib = None
+
+
+def build() -> Path:
+    src = HERE / "oracle.c"
+    if not LIB.exists() or LIB.stat().st_mtime < src.stat().st_mtime:
+        subprocess.run(["make", "-s", "-C", str(HERE), "liboracle.so"], check=True)
+    return LIB
+
+
+def load():
+    global _lib
+    if _lib is None:
+        build()
+        lib = C.CDLL(str(LIB))
+        u32p, i32p = C.POINTER(C.c_uint32), C.POINTER(C.c_int32)
+        lib.orc_gr_read.restype = C.c_int
+        lib.orc_gr_read.argtypes = [C.c_char_p, u32p, u32p, C.POINTER(u32p), C.POINTER(u32p), C.POINTER(i32p)]
+        lib.orc_free.argtypes = [C.c_void_p]
+        lib.orc_bfs.restype = C.c_uint64
+        lib.orc_bfs.argtypes = [C.c_uint32, C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p]
+        lib.orc_sssp.restype = C.c_int64
+        lib.orc_sssp.argtypes = [C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p]
+        lib.orc_check_tree.restype = C.c_uint64
+        lib.orc_check_tree.argtypes = [C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p,
+                                       C.c_void_p]
+        lib.orc_reach_stats.argtypes = [C.c_uint32, C.c_void_p, C.c_void_p, C.POINTER(C.c_uint64),
+                                        C.POINTER(C.c_uint64)]
+        lib.orc_write_output.restype = C.c_int
+        lib.orc_write_output.argtypes = [C.c_char_p, C.c_uint32, C.c_void_p]
+        lib.orc_read_output.restype = C.c_int64
+        lib.orc_read_output.argtypes = [C.c_char_p, C.c_uint32, C.c_void_p]
+        _lib = lib
+    return _lib
+
+
+def _p(a):
+    return C.c_void_p(a.ctypes.data) if a is not None else C.c_void_p(0)
+
+
+def gr_read(path: str | os.PathLike):
+    """Returns (row_start, edge_dst, edge_data or None); raises on a parse error."""
+    lib = load()
+    n, m = C.c_uint32(), C.c_uint32()
+    rs, dst = C.POINTER(C.c_uint32)(), C.POINTER(C.c_uint32)()
+    w = C.POINTER(C.c_int32)()
+    r = lib.orc_gr_read(str(path).encode(), C.byref(n), C.byref(m), C.byref(rs), C.byref(dst), C.byref(w))
+    if r != 0:
+        raise ValueError(f"oracle: cannot parse {path} (code {r})")
+    try:
+        a_rs = np.ctypeslib.as_array(rs, shape=(n.value + 1,)).copy()
+        a_dst = np.ctypeslib.as_array(dst, shape=(max(m.value, 1),))[: m.value].copy()
+        a_w = np.ctypeslib.as_array(w, shape=(max(m.value, 1),))[: m.value].copy() if w else None
+    finally:
+        lib.orc_free(C.cast(rs, C.c_void_p))
+        lib.orc_free(C.cast(dst, C.c_void_p))
+        if w:
+            lib.orc_free(C.cast(w, C.c_void_p))
+    return a_rs, a_dst, a_w
+
+
+def bfs(row_start, edge_dst, src: int, parent: bool = False):
+    rs = np.ascontiguousarray(row_start, dtype=np.uint32)
+    dst = np.ascontiguousarray(edge_dst, dtype=np.uint32)
+    n = len(rs) - 1
+    level = np.empty(n, dtype=np.int32)
+    par = np.empty(n, dtype=np.uint32) if parent else None
+    load().orc_bfs(n, _p(rs), _p(dst), src, _p(level), _p(par))
+    return (level, par) if parent else level
+
+
+def sssp(row_start, edge_dst, edge_data, src: int, parent: bool = False):
+    """Dijkstra; edge_data None means every weight is 0 (as the reference's
+    calloc'd edge_data for an unweighted .gr)."""
+    rs = np.ascontiguousarray(row_start, dtype=np.uint32)
+    dst = np.ascontiguousarray(edge_dst, dtype=np.uint32)
+    w = (np.zeros(len(dst), dtype=np.int32) if edge_data is None
+         else np.ascontiguousarray(edge_data, dtype=np.int32))
+    n = len(rs) - 1
+    dist = np.empty(n, dtype=np.int32)
+    par = np.empty(n, dtype=np.uint32) if parent else None
+    r = load().orc_sssp(n, _p(rs), _p(dst), _p(w), src, _p(dist), _p(par))
+    if r < 0:
+        raise OverflowError("oracle: a shortest-path distance exceeds INT_MAX - 1")
+    return (dist, par) if parent else dist
+
+
+def check_tree(row_start, edge_dst, edge_data, src: int, values, parent) -> int:
+    """Number of parent-tree violations (0 = valid); edge_data None = BFS."""
+    rs = np.ascontiguousarray(row_start, dtype=np.uint32)
+    dst = np.ascontiguousarray(edge_dst, dtype=np.uint32)
+    w = None if edge_data is None else np.ascontiguousarray(edge_data, dtype=np.int32)
+    v = np.ascontiguousarray(values, dtype=np.int32)
+    p = np.ascontiguousarray(parent, dtype=np.uint32)
+    return int(load().orc_check_tree(len(rs) - 1, _p(rs), _p(dst), _p(w), src, _p(v), _p(p)))
+
+
+def reach_stats(row_start, values) -> tuple[int, int]:
+    rs = np.ascontiguousarray(row_start, dtype=np.uint32)
+    v = np.ascontiguousarray(values, dtype=np.int32)
+    vr, er = C.c_uint64(), C.c_uint64()
+    load().orc_reach_stats(len(rs) - 1, _p(rs), _p(v), C.byref(vr), C.byref(er))
+    return vr.value, er.value
+
+
+def write_output(path, values) -> None:
+    v = np.ascontiguousarray(values, dtype=np.int32)
+    if load().orc_write_output(str(path).encode(), len(v), _p(v)) != 0:
+        raise OSError(f"oracle: cannot write {path}")
+
+
+def read_output(path, nnodes: int) -> np.ndarray:
+    v = np.full(nnodes, -1, dtype=np.int32)
+    r = load().orc_read_output(str(path).encode(), nnodes, _p(v))
+    if r != nnodes:
+        raise ValueError(f"oracle: {path}: parsed {r} lines, expected {nnodes}")
+    return v

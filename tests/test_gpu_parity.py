@@ -1,0 +1,164 @@
+"""GPU parity: libgft BFS / SSSP (through the C ABI) against the CPU oracle,
+bit for bit, plus parent-tree validity, on hand graphs and seeded synthetic
+graphs at sizes the oracle finishes in seconds."""
+
+import numpy as np
+import pytest
+
+from graphs import hand_cases
+
+pytestmark = pytest.mark.gpu
+
+TUNES = [
+    dict(),
+    dict(block_threads=256, blocks_per_sm=4),
+    dict(block_threads=1024, blocks_per_sm=1),
+    dict(hub_degree=32),  # every vertex of degree >= 32 goes through the grid-wide hub phase
+]
+
+
+def _sources(n):
+    return sorted({0, n // 2, n - 1})
+
+
+def _run_bfs(gft, engine, dg, src, tune=None):
+    import torch
+
+    par = torch.empty(dg.nnodes, dtype=torch.int32, device="cuda")
+    r = engine.bfs(dg, src, parent=par, tune=gft.Tune(**tune) if tune else None)
+    return r["out"].cpu().numpy(), r["parent"].cpu().numpy().view(np.uint32), r
+
+
+def _run_sssp(gft, engine, dg, src, delta, tune=None):
+    import torch
+
+    par = torch.empty(dg.nnodes, dtype=torch.int32, device="cuda")
+    r = engine.sssp(dg, src, delta=delta, parent=par, tune=gft.Tune(**tune) if tune else None)
+    return r["out"].cpu().numpy(), r["parent"].cpu().numpy().view(np.uint32), r
+
+
+@pytest.mark.parametrize("case", hand_cases(), ids=lambda c: c[0])
+def test_hand_graphs_bfs_sssp(gft, orc, engine, case):
+    name, rs, dst, w = case
+    g = gft.CSRGraph(rs, dst, w)
+    dg = g.copy_to_gpu()
+    for src in _sources(g.nnodes):
+        want = orc.bfs(rs, dst, src)
+        got, par, _ = _run_bfs(gft, engine, dg, src)
+        np.testing.assert_array_equal(got, want)
+        assert orc.check_tree(rs, dst, None, src, got, par) == 0
+        for delta in (1, 7, 10000):
+            want = orc.sssp(rs, dst, w, src)
+            got, par, _ = _run_sssp(gft, engine, dg, src, delta)
+            np.testing.assert_array_equal(got, want)
+            if w is not None and (w > 0).all():
+                assert orc.check_tree(rs, dst, w, src, got, par) == 0
+
+
+@pytest.mark.parametrize("tune", TUNES, ids=lambda t: ",".join(f"{k}={v}" for k, v in t.items()) or "default")
+def test_grid_bfs_closed_form(gft, orc, engine, tune):
+    g = gft.CSRGraph.grid(256, 256)
+    dg = g.copy_to_gpu()
+    got, par, st = _run_bfs(gft, engine, dg, 0, tune)
+    r, c = np.divmod(np.arange(g.nnodes), 256)
+    np.testing.assert_array_equal(got, (r + c).astype(np.int32))
+    assert orc.check_tree(g.row_start, g.edge_dst, None, 0, got, par) == 0
+    assert st["levels"] == 511
+
+
+@pytest.mark.parametrize("tune", TUNES, ids=lambda t: ",".join(f"{k}={v}" for k, v in t.items()) or "default")
+def test_rmat_bfs_sssp(gft, orc, engine, tune):
+    g = gft.CSRGraph.rmat(16, 16, seed=3, max_weight=255)
+    dg = g.copy_to_gpu()
+    for src in g.pick_sources(2, 3):
+        want = orc.bfs(g.row_start, g.edge_dst, src)
+        got, par, _ = _run_bfs(gft, engine, dg, src, tune)
+        np.testing.assert_array_equal(got, want)
+        assert orc.check_tree(g.row_start, g.edge_dst, None, src, got, par) == 0
+        want = orc.sssp(g.row_start, g.edge_dst, g.edge_data, src)
+        for delta in (16, 255, 10000):
+            got, par, _ = _run_sssp(gft, engine, dg, src, delta, tune)
+            np.testing.assert_array_equal(got, want)
+            assert orc.check_tree(g.row_start, g.edge_dst, g.edge_data, src, got, par) == 0
+
+
+def test_road_sssp(gft, orc, engine):
+    g = gft.CSRGraph.road(512, seed=1)
+    dg = g.copy_to_gpu()
+    for src in g.pick_sources(1, 2):
+        want = orc.sssp(g.row_start, g.edge_dst, g.edge_data, src)
+        for delta in (1000, 10000, 100000):
+            got, par, st = _run_sssp(gft, engine, dg, src, delta)
+            np.testing.assert_array_equal(got, want)
+            assert orc.check_tree(g.row_start, g.edge_dst, g.edge_data, src, got, par) == 0
+
+
+def test_unweighted_sssp_is_zero_weight(gft, orc, engine):
+    """An unweighted .gr has weight 0 everywhere (calloc'd edge_data in the
+    reference), so every reached vertex has distance 0."""
+    g = gft.CSRGraph.rmat(12, 8, seed=5)
+    dg = g.copy_to_gpu()
+    src = g.pick_sources(1, 1)[0]
+    got, _, _ = _run_sssp(gft, engine, dg, src, 10000)
+    np.testing.assert_array_equal(got, orc.sssp(g.row_start, g.edge_dst, None, src))
+
+
+@pytest.mark.parametrize(
+    "kind,kw,host",
+    [
+        ("grid", dict(rows=100, cols=37, max_weight=1), lambda g: g.CSRGraph.grid(100, 37, 1, 1)),
+        ("road", dict(side=300), lambda g: g.CSRGraph.road(300, seed=1)),
+        ("rmat", dict(scale=14, edge_factor=16, max_weight=255), lambda g: g.CSRGraph.rmat(14, 16, seed=1, max_weight=255)),
+        ("rmat", dict(scale=12, edge_factor=8), lambda g: g.CSRGraph.rmat(12, 8, seed=1)),
+    ],
+)
+def test_device_generator_matches_host(gft, kind, kw, host):
+    dg = gft.DeviceGraph.generate(kind, seed=1, **kw)
+    a = dg.download()
+    b = host(gft)
+    np.testing.assert_array_equal(a.row_start, b.row_start)
+    np.testing.assert_array_equal(a.edge_dst, b.edge_dst)
+    if b.edge_data is None:
+        assert a.edge_data is None
+    else:
+        np.testing.assert_array_equal(a.edge_data, b.edge_data)
+
+
+def test_host_api_matches_device_api(gft, orc, engine):
+    g = gft.CSRGraph.road(128, seed=4)
+    dg = g.copy_to_gpu()
+    out = np.empty(g.nnodes, dtype=np.int32)
+    par = np.empty(g.nnodes, dtype=np.uint32)
+    engine.sssp_host(dg, 5, out, parent=par)
+    np.testing.assert_array_equal(out, orc.sssp(g.row_start, g.edge_dst, g.edge_data, 5))
+    assert orc.check_tree(g.row_start, g.edge_dst, g.edge_data, 5, out, par) == 0
+    engine.bfs_host(dg, 5, out, parent=par)
+    np.testing.assert_array_equal(out, orc.bfs(g.row_start, g.edge_dst, 5))
+    assert orc.check_tree(g.row_start, g.edge_dst, None, 5, out, par) == 0
+
+
+def test_barrier_timeout_is_reported_and_engine_recovers(gft, orc, engine):
+    """One CTA never arrives at the first grid barrier (test hook); the other
+    CTAs' bounded waits expire, the call returns GFT_ERR_TIMEOUT and the
+    context stays usable."""
+    g = gft.CSRGraph.grid(64, 64)
+    dg = g.copy_to_gpu()
+    with pytest.raises(gft.GftError) as ei:
+        engine.bfs(dg, 0, tune=gft.Tune(timeout_ms=200, test_skip_block=1))
+    assert ei.value.status_name == "GFT_ERR_TIMEOUT"
+    with pytest.raises(gft.GftError) as ei:
+        engine.sssp(dg, 0, tune=gft.Tune(timeout_ms=200, test_skip_block=0))
+    assert ei.value.status_name == "GFT_ERR_TIMEOUT"
+    r = engine.bfs(dg, 0)
+    np.testing.assert_array_equal(r["out"].cpu().numpy(), orc.bfs(g.row_start, g.edge_dst, 0))
+
+
+def test_invalid_arguments(gft, engine):
+    g = gft.CSRGraph.grid(8, 8)
+    dg = g.copy_to_gpu()
+    with pytest.raises(gft.GftError, match="INVALID_ARG"):
+        engine.bfs(dg, 64)
+    with pytest.raises(gft.GftError, match="INVALID_ARG"):
+        engine.sssp(dg, 0, delta=0)
+    with pytest.raises(gft.GftError, match="INVALID_ARG"):
+        engine.bfs(dg, 0, tune=gft.Tune(block_threads=300))
