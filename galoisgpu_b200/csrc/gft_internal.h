@@ -65,6 +65,7 @@ struct alignas(128) CtlLine {
 
 struct TraversalCtl {
     CtlLine barrier;       // grid barrier arrival counter (u64)
+    CtlLine release;       // grid barrier release flag: last completed episode (u32)
     CtlLine qlen[3];       // frontier (SSSP: near pile) length per iteration slot (u32)
     CtlLine claim[3];      // work-claim cursor per iteration slot (u32)
     CtlLine hub[3];        // (hubs << 32) | hub chunks per iteration slot (u64)

@@ -216,19 +216,35 @@ __device__ __forceinline__ void warp_range(Vis &vis, uint32_t start, uint32_t le
     }
 }
 
-// Expands the frontier `in[0, n)`: warps claim `grain` vertices at a time.
-// Vertices of degree >= hub_degree are recorded in the hub list for the
-// grid-wide hub phase instead.
+// Chunk schedule shared by every grid-wide loop: chunk c covers items
+// [c * grain, (c + 1) * grain).  Warp w first takes chunk w with no atomic;
+// only when there are more chunks than warps do warps claim further chunks
+// from the iteration's cursor (one atomic per chunk).  A small frontier
+// therefore costs no atomics at all.
+struct ChunkSched {
+    unsigned nchunks, nwarps, gwarp, lane;
+    unsigned *cursor;
+    __device__ __forceinline__ unsigned first() const { return gwarp; }
+    __device__ __forceinline__ unsigned next() const
+    {
+        if (nchunks <= nwarps) return nchunks;
+        unsigned c = 0;
+        if (lane == 0) c = nwarps + atomicAdd(cursor, 1u);
+        return __shfl_sync(kFull, c, 0);
+    }
+};
+
+// Expands the frontier `in[0, n)` in chunks of `grain` vertices.  Vertices
+// of degree >= hub_degree are recorded in the hub list for the grid-wide hub
+// phase instead.
 template <class Vis, class Own>
 __device__ __forceinline__ void expand_frontier(Vis &vis, const TravParams &p, const uint32_t *in, uint32_t n,
                                                 unsigned *claim, unsigned long long *hub_ctr, unsigned grain,
-                                                unsigned lane)
+                                                unsigned gwarp, unsigned nwarps, unsigned lane)
 {
-    for (;;) {
-        unsigned base = 0;
-        if (lane == 0) base = atomicAdd(claim, grain);
-        base = __shfl_sync(kFull, base, 0);
-        if (base >= n) break;
+    const ChunkSched cs{(n + grain - 1) / grain, nwarps, gwarp, lane, claim};
+    for (unsigned c = cs.first(); c < cs.nchunks; c = cs.next()) {
+        const unsigned base = c * grain;
         const unsigned end = min(n, base + grain);
         for (unsigned i0 = base; i0 < end; i0 += 32) {
             const unsigned idx = i0 + lane;
@@ -265,13 +281,10 @@ __device__ __forceinline__ void expand_frontier(Vis &vis, const TravParams &p, c
 // kHubChunk-edge chunks; hub h owns chunks [hubs[h].y, hubs[h+1].y).
 template <class Vis, class Own>
 __device__ __forceinline__ void expand_hubs(Vis &vis, const TravParams &p, unsigned nh, unsigned nc,
-                                            unsigned *hub_claim, unsigned lane)
+                                            unsigned *hub_claim, unsigned gwarp, unsigned nwarps, unsigned lane)
 {
-    for (;;) {
-        unsigned c = 0;
-        if (lane == 0) c = atomicAdd(hub_claim, 1u);
-        c = __shfl_sync(kFull, c, 0);
-        if (c >= nc) break;
+    const ChunkSched cs{nc, nwarps, gwarp, lane, hub_claim};
+    for (unsigned c = cs.first(); c < nc; c = cs.next()) {
         unsigned lo = 0, hi = nh;
         while (hi - lo > 1) {
             unsigned mid = (lo + hi) >> 1;
@@ -281,7 +294,7 @@ __device__ __forceinline__ void expand_hubs(Vis &vis, const TravParams &p, unsig
         const uint2 hb = __ldcg(p.hubs + lo);
         const uint32_t u = hb.x;
         Own o = vis.owner(true, u);
-        if (!vis.active(o)) continue;
+        if (!vis.active(o)) continue;  // warp uniform: every lane read the same hub
         const uint32_t start = __ldg(p.row_start + u);
         const uint32_t deg = __ldg(p.row_start + u + 1) - start;
         const uint32_t off = (c - hb.y) * kHubChunk;
@@ -309,8 +322,8 @@ __global__ void __launch_bounds__(BLOCK) bfs_persistent(TravParams p)
 
     const unsigned lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const unsigned tid = blockIdx.x * BLOCK + threadIdx.x, nthreads = gridDim.x * BLOCK;
-    const unsigned nwarps = nthreads / 32;
-    GridSync gs{&ctl->barrier.v, &ctl->error, &ctl->error_where, gridDim.x, 0, p.timeout_ns};
+    const unsigned nwarps = nthreads / 32, gwarp = tid / 32;
+    GridSync gs{&ctl->barrier.v, u32_of(ctl->release), &ctl->error, &ctl->error_where, gridDim.x, 0, p.timeout_ns};
 
     // Initialise (apps/bfs/kernel.cu:20-32): level 0 at src, INF elsewhere.
     const uint32_t n = p.nnodes, nwords = (n + 31) >> 5;
@@ -355,13 +368,13 @@ __global__ void __launch_bounds__(BLOCK) bfs_persistent(TravParams p)
         vis.q.queue = p.q[(L + 1) & 1];
         vis.q.len = u32_of(ctl->qlen[nslot]);
         expand_frontier<BfsVisitor, BfsOwn>(vis, p, p.q[L & 1], n_in, u32_of(ctl->claim[slot]), &ctl->hub[slot].v,
-                                            pick_grain(n_in, nwarps), lane);
+                                            pick_grain(n_in, nwarps), gwarp, nwarps, lane);
         vis.q.flush(lane);
         if (!gs.sync()) return;
         const unsigned long long hv = ld_relaxed_u64(&ctl->hub[slot].v);
         if (hv) {
             expand_hubs<BfsVisitor, BfsOwn>(vis, p, (unsigned)(hv >> 32), (unsigned)hv, u32_of(ctl->hub_claim[slot]),
-                                            lane);
+                                            gwarp, nwarps, lane);
             vis.q.flush(lane);
             if (!gs.sync()) return;
         }
@@ -389,8 +402,8 @@ __global__ void __launch_bounds__(BLOCK) sssp_persistent(TravParams p)
 
     const unsigned lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const unsigned tid = blockIdx.x * BLOCK + threadIdx.x, nthreads = gridDim.x * BLOCK;
-    const unsigned nwarps = nthreads / 32;
-    GridSync gs{&ctl->barrier.v, &ctl->error, &ctl->error_where, gridDim.x, 0, p.timeout_ns};
+    const unsigned nwarps = nthreads / 32, gwarp = tid / 32;
+    GridSync gs{&ctl->barrier.v, u32_of(ctl->release), &ctl->error, &ctl->error_where, gridDim.x, 0, p.timeout_ns};
     unsigned *dist = reinterpret_cast<unsigned *>(p.out);
 
     // Initialise (apps/sssp/kernel.cu:23-35): 0 at src, INF elsewhere.
@@ -447,7 +460,7 @@ __global__ void __launch_bounds__(BLOCK) sssp_persistent(TravParams p)
             vis.fq.queue = p.far[P & 1];
             vis.fq.len = u32_of(ctl->far_len[P % 3]);
             expand_frontier<SsspVisitor, SsspOwn>(vis, p, p.q[I & 1], n_near, u32_of(ctl->claim[slot]),
-                                                  &ctl->hub[slot].v, pick_grain(n_near, nwarps), lane);
+                                                  &ctl->hub[slot].v, pick_grain(n_near, nwarps), gwarp, nwarps, lane);
             vis.nq.flush(lane);
             vis.fq.flush(lane);
             unsigned fm = warp_min_u32(vis.far_min);
@@ -457,7 +470,7 @@ __global__ void __launch_bounds__(BLOCK) sssp_persistent(TravParams p)
             if (hv) {
                 vis.far_min = kInf;
                 expand_hubs<SsspVisitor, SsspOwn>(vis, p, (unsigned)(hv >> 32), (unsigned)hv,
-                                                  u32_of(ctl->hub_claim[slot]), lane);
+                                                  u32_of(ctl->hub_claim[slot]), gwarp, nwarps, lane);
                 vis.nq.flush(lane);
                 vis.fq.flush(lane);
                 fm = warp_min_u32(vis.far_min);
@@ -481,12 +494,11 @@ __global__ void __launch_bounds__(BLOCK) sssp_persistent(TravParams p)
             vis.fq.len = u32_of(ctl->far_len[(P + 1) % 3]);
             const uint32_t *pile = p.far[P & 1];
             unsigned local_min = kInf;
-            for (;;) {
-                unsigned base = 0;
-                if (lane == 0) base = atomicAdd(u32_of(ctl->claim[slot]), 32u * 4u);
-                base = __shfl_sync(kFull, base, 0);
-                if (base >= nf) break;
-                const unsigned end = min(nf, base + 128u);
+            const unsigned sgrain = pick_grain(nf, nwarps);
+            const ChunkSched cs{(nf + sgrain - 1) / sgrain, nwarps, gwarp, lane, u32_of(ctl->claim[slot])};
+            for (unsigned c = cs.first(); c < cs.nchunks; c = cs.next()) {
+                const unsigned base = c * sgrain;
+                const unsigned end = min(nf, base + sgrain);
                 for (unsigned i0 = base; i0 < end; i0 += 32) {
                     const unsigned idx = i0 + lane;
                     uint32_t v = 0;

@@ -55,9 +55,23 @@ __device__ __forceinline__ unsigned long long ld_relaxed_u64(const unsigned long
     return v;
 }
 
-__device__ __forceinline__ void red_release_add_u64(unsigned long long *p, unsigned long long v)
+__device__ __forceinline__ unsigned long long atom_add_acq_rel_u64(unsigned long long *p, unsigned long long v)
 {
-    asm volatile("red.release.gpu.global.add.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+    unsigned long long old;
+    asm volatile("atom.acq_rel.gpu.global.add.u64 %0, [%1], %2;" : "=l"(old) : "l"(p), "l"(v) : "memory");
+    return old;
+}
+
+__device__ __forceinline__ void st_release_u32(unsigned *p, unsigned v)
+{
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned *p)
+{
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
 }
 
 __device__ __forceinline__ unsigned lanemask_lt()
@@ -73,14 +87,18 @@ __device__ __forceinline__ void raise_error(unsigned *err, unsigned *where, unsi
     if (atomicCAS(err, 0u, code) == 0u) atomicExch(where, site);
 }
 
-// Grid barrier over a cooperative launch.  Arrivals count up on one 64-bit
-// counter; episode k is complete when the counter reaches k * nblocks, so the
-// counter never needs resetting inside the launch.  Thread 0 of each CTA
-// waits with a bounded spin (globaltimer); on expiry it records
-// GFT_ERR_TIMEOUT, and every waiter also leaves as soon as any CTA has
-// recorded an error, so no CTA can be left spinning.
+// Grid barrier over a cooperative launch.  Thread 0 of every CTA arrives
+// with one acq_rel atomic on a monotonic 64-bit counter (episode k is
+// complete when it reaches k * nblocks, so it is never reset inside a
+// launch).  The CTA whose arrival completes the episode publishes k on a
+// separate release flag; the others poll that flag (in its own 128-byte
+// line, so polling does not contend with the arrival atomics).  Each wait is
+// bounded (globaltimer): on expiry the CTA records GFT_ERR_TIMEOUT, and every
+// waiter also leaves as soon as any CTA has recorded an error, so no CTA can
+// be left spinning.
 struct GridSync {
     unsigned long long *counter;
+    unsigned *flag;
     unsigned *error;
     unsigned *error_where;
     unsigned nblocks;
@@ -94,19 +112,23 @@ struct GridSync {
         __syncthreads();
         if (threadIdx.x == 0) {
             epoch++;
-            unsigned long long target = (unsigned long long)epoch * nblocks;
+            const unsigned long long target = (unsigned long long)epoch * nblocks;
             __threadfence();
-            red_release_add_u64(counter, 1ull);
-            unsigned long long t0 = 0;
-            unsigned spins = 0;
-            while (ld_acquire_u64(counter) < target) {
-                if (ld_relaxed_u32(error)) break;
-                if ((++spins & 127u) == 0) {
-                    unsigned long long now = globaltimer_ns();
-                    if (t0 == 0) t0 = now;
-                    else if (now - t0 > timeout_ns) {
-                        raise_error(error, error_where, GFT_ERR_TIMEOUT, epoch);
-                        break;
+            const unsigned long long old = atom_add_acq_rel_u64(counter, 1ull);
+            if (old + 1 == target) {
+                st_release_u32(flag, epoch);
+            } else {
+                unsigned long long t0 = 0;
+                unsigned spins = 0;
+                while ((int)(ld_acquire_u32(flag) - epoch) < 0) {
+                    if (ld_relaxed_u32(error)) break;
+                    if ((++spins & 127u) == 0) {
+                        unsigned long long now = globaltimer_ns();
+                        if (t0 == 0) t0 = now;
+                        else if (now - t0 > timeout_ns) {
+                            raise_error(error, error_where, GFT_ERR_TIMEOUT, epoch);
+                            break;
+                        }
                     }
                 }
             }

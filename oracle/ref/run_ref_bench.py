@@ -1,0 +1,100 @@
+"""Times the reference's own CUDA build (oracle/_ref, built by
+oracle/ref/Makefile from the reference sources) on the full-size seeded
+configurations, the way a user runs it: ``bfs|sssp -q -s <src> [-d delta]
+<graph.gr>``, one process per query, reading its ``Total time: N ns`` line
+(reference skelapp/skel.cu:159-166; that time includes the worklist
+allocations gg_main makes, apps/bfs/kernel.cu:389, apps/sssp/kernel.cu:475).
+Kernel-only time comes from running this same script under
+``ncu --metrics gpu__time_duration.sum -k regex:gg_main_pipe``.
+
+Test/measurement infrastructure only: the input graphs are produced with this
+repository's generator, and E_r comes from this repository's engine (whose
+reach sets equal the reference's, checked with --check).
+
+    python oracle/ref/run_ref_bench.py --config road4096 --sources 1 --check
+"""
+
+from __future__ import annotations
+
+import argparse
+import hashlib
+import json
+import os
+import re
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parents[2]
+sys.path.insert(0, str(ROOT))
+
+import numpy as np  # noqa: E402
+
+import galoisgpu_b200 as gft  # noqa: E402
+from oracle import oracle as orc  # noqa: E402
+
+REF = ROOT / "oracle" / "_ref"
+CONFIGS = {
+    "grid256": dict(kind="grid", kw=dict(rows=256, cols=256, max_weight=1), seed=0, app="bfs", src_seed=None),
+    "road4096": dict(kind="road", kw=dict(side=4096), seed=1, app="sssp", src_seed=1, delta=10000),
+    "rmat24": dict(kind="rmat", kw=dict(scale=24, edge_factor=16), seed=1, app="bfs", src_seed=2),
+    "road1024": dict(kind="road", kw=dict(side=1024), seed=1, app="sssp", src_seed=1, delta=10000),
+    "rmat20": dict(kind="rmat", kw=dict(scale=20, edge_factor=16), seed=1, app="bfs", src_seed=2),
+}
+
+
+def main(argv=None) -> int:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--config", choices=sorted(CONFIGS), required=True)
+    ap.add_argument("--sources", type=int, default=1)
+    ap.add_argument("--delta", type=int, default=None)
+    ap.add_argument("--workdir", default=os.environ.get("TMPDIR", tempfile.gettempdir()))
+    ap.add_argument("--check", action="store_true", help="compare the reference output with this engine's")
+    a = ap.parse_args(argv)
+    c = CONFIGS[a.config]
+    dg = gft.DeviceGraph.generate(c["kind"], seed=c["seed"], **c["kw"])
+    host = dg.download()
+    srcs = [0] if c["src_seed"] is None else host.pick_sources(c["src_seed"], a.sources)
+    gr = Path(a.workdir) / f"gft_{a.config}.gr"
+    t0 = time.time()
+    host.write(gr)
+    sha = hashlib.sha256(gr.read_bytes()).hexdigest()[:16]
+    print(f"wrote {gr} ({gr.stat().st_size / 1e9:.2f} GB, sha256 {sha}) in {time.time() - t0:.1f}s",
+          file=sys.stderr, flush=True)
+    eng = gft.Engine(0)
+    delta = a.delta or c.get("delta")
+    results = []
+    for i, s in enumerate(srcs):
+        mine = (eng.sssp(dg, s, delta=delta) if c["app"] == "sssp" else eng.bfs(dg, s))["out"]
+        v_r, e_r = gft.reach_stats(dg, mine)
+        out = Path(a.workdir) / f"gft_{a.config}.s{s}.out"
+        check = a.check and i == 0
+        cmd = [str(REF / c["app"]), "-s", str(s)]
+        if c["app"] == "sssp":
+            cmd += ["-d", str(delta)]
+        cmd += ["-o", str(out)] if check else ["-q"]
+        cmd.append(str(gr))
+        t = time.time()
+        r = subprocess.run(cmd, capture_output=True, text=True, timeout=1800)
+        wall = time.time() - t
+        if r.returncode != 0:
+            print(r.stdout, r.stderr, file=sys.stderr)
+            return r.returncode
+        m = re.search(r"Total time: (\d+) ns", r.stderr)
+        ns = int(m.group(1)) if m else None
+        rec = {"config": a.config, "app": c["app"], "src": s, "delta": delta, "total_time_ns": ns,
+               "gteps_total_time": e_r / ns if ns else None, "E_r": e_r, "V_r": v_r, "process_wall_s": wall}
+        if check:
+            ref = orc.read_output(out, host.nnodes)
+            rec["parity_vs_gft"] = "bit-exact" if np.array_equal(ref, mine.cpu().numpy()) else "MISMATCH"
+            out.unlink()
+        results.append(rec)
+        print(json.dumps(rec), flush=True)
+    gr.unlink()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())
