@@ -73,49 +73,6 @@ def log(*a):
 
 
 # ---------------------------------------------------------------------------
-# distributed plumbing
-# ---------------------------------------------------------------------------
-class Dist:
-    def __init__(self, n_gpus: int):
-        self.world = int(os.environ.get("WORLD_SIZE", "1"))
-        self.rank = int(os.environ.get("RANK", "0"))
-        self.local = int(os.environ.get("LOCAL_RANK", "0"))
-        self.pg = None
-        if self.world > 1:
-            import datetime
-
-            import torch
-            import torch.distributed as dist
-
-            os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
-            torch.cuda.set_device(self.local)
-            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
-                                    device_id=torch.device("cuda", self.local))
-            self.pg = dist
-
-    def barrier(self):
-        if self.pg:
-            import torch
-
-            t = torch.zeros(1, device="cuda")
-            self.pg.all_reduce(t)
-            torch.cuda.synchronize()
-
-    def max(self, x: float) -> float:
-        if not self.pg:
-            return x
-        import torch
-
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
-        return float(t.item())
-
-    def close(self):
-        if self.pg:
-            self.pg.destroy_process_group()
-
-
-# ---------------------------------------------------------------------------
 # clocks
 # ---------------------------------------------------------------------------
 class ClockSampler:
@@ -259,7 +216,7 @@ def run_queries(gft, eng, dg, spec, sources, out, stream):
     return kms
 
 
-def bench_workload(gft, name: str, steps: int, warmup: int, d: Dist, dev: int, headline: bool) -> dict:
+def bench_workload(gft, name: str, steps: int, warmup: int, d, dev: int, headline: bool):
     import torch
 
     spec = WORKLOADS[name]
@@ -372,7 +329,9 @@ def our_arm(args) -> int:
 
     import galoisgpu_b200 as gft
 
-    d = Dist(args.gpus)
+    from galoisgpu_b200.replicas import ReplicaGroup
+
+    d = ReplicaGroup()
     dev = d.local if d.world > 1 else 0
     torch.cuda.set_device(dev)
     name = args.workload

@@ -118,10 +118,11 @@ def build(force: bool = False, verbose: bool = False, ptxas_verbose: bool = Fals
         os.replace(tmp, LIB)
     cli_src = CSRC / CLI_SOURCE
     if cli_src.exists():
-        cli_obj = BUILD / (CLI_SOURCE + ".o")
-        if force or _newer(cli_obj, [cli_src, INCLUDE / "gft.h"]):
-            _compile(cli_src, cli_obj, verbose, False)
         for app in ("bfs", "sssp"):
+            cli_obj = BUILD / f"cli_{app}.o"
+            if force or _newer(cli_obj, [cli_src, INCLUDE / "gft.h"]):
+                _run(["g++", *CXX_FLAGS, f"-DGFT_APP_SSSP={int(app == 'sssp')}", "-c", str(cli_src), "-o",
+                      str(cli_obj)], verbose)
             exe = BIN / app
             if force or _newer(exe, [cli_obj, LIB]):
                 _run(

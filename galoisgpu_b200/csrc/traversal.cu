@@ -21,6 +21,8 @@
 //     but splits the far pile by threshold with per-vertex phase stamps
 //     (no separate duplicate-removal pass, apps/sssp/kernel.cu:36-66) and
 //     skips empty buckets.
+#include <string.h>
+
 #include <algorithm>
 
 #include "gft_internal.h"
@@ -585,9 +587,13 @@ __global__ void reach_stats_kernel(const uint32_t *__restrict__ row_start, const
 // ---------------------------------------------------------------------------
 namespace {
 
-constexpr uint32_t kDefaultBlock = 512;
+// Defaults from the autotuner on a B200 (RMAT-24 BFS, RMAT-20 SSSP and the
+// 4096^2 road grid): 1024-thread CTAs for BFS, 512 for SSSP, two CTAs per
+// SM, and vertices of degree >= 256 split across the grid.
+constexpr uint32_t kDefaultBlockBfs = 1024;
+constexpr uint32_t kDefaultBlockSssp = 512;
 constexpr uint32_t kDefaultBlocksPerSm = 2;
-constexpr uint32_t kDefaultHubDegree = 4096;
+constexpr uint32_t kDefaultHubDegree = 256;
 constexpr uint32_t kDefaultTimeoutMs = 20000;
 
 const void *bfs_kernel_for(int block)
@@ -615,9 +621,10 @@ struct Tune {
     int skip;
 };
 
-Tune resolve_tuning(const gft_tuning *t)
+Tune resolve_tuning(const gft_tuning *t, bool is_sssp)
 {
-    Tune r{kDefaultBlock, kDefaultBlocksPerSm, kDefaultHubDegree, kDefaultTimeoutMs, -1};
+    Tune r{is_sssp ? kDefaultBlockSssp : kDefaultBlockBfs, kDefaultBlocksPerSm, kDefaultHubDegree, kDefaultTimeoutMs,
+           -1};
     if (t) {
         if (t->block_threads) r.block = t->block_threads;
         if (t->blocks_per_sm) r.bps = t->blocks_per_sm;
@@ -666,7 +673,7 @@ gft_status run_traversal(bool is_sssp, gft_engine *e, const gft_graph *g, uint32
     if (!d_out) return fail(GFT_ERR_INVALID_ARG, "%s: output pointer is NULL", what);
     if (src >= G.nnodes) return fail(GFT_ERR_INVALID_ARG, "%s: source %u out of range (nnodes %u)", what, src, G.nnodes);
     if (is_sssp && delta <= 0) return fail(GFT_ERR_INVALID_ARG, "%s: delta must be > 0 (got %d)", what, delta);
-    Tune t = resolve_tuning(tune);
+    Tune t = resolve_tuning(tune, is_sssp);
     const void *kern = is_sssp ? sssp_kernel_for(t.block) : bfs_kernel_for(t.block);
     if (!kern) return fail(GFT_ERR_INVALID_ARG, "%s: block_threads must be 256, 512 or 1024", what);
     if (t.hub < 32) t.hub = 32;
@@ -820,3 +827,4 @@ gft_status gft_reach_stats(const gft_graph *g, const int32_t *d_val, void *strea
 }
 
 }  // extern "C"
+
