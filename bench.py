@@ -62,9 +62,26 @@ WORKLOADS = {
     "bfs-grid-256": dict(kind="grid", rows=256, cols=256, seed=0, app="bfs", nsrc=0, src_seed=0),
     # Smaller cases of the same kernels (profiling captures).
     "sssp-road-1024": dict(kind="road", side=1024, seed=1, app="sssp", delta=10000, nsrc=1, src_seed=1),
+    "sssp-road-2048": dict(kind="road", side=2048, seed=1, app="sssp", delta=10000, nsrc=1, src_seed=1),
     "bfs-rmat-20": dict(kind="rmat", scale=20, edge_factor=16, seed=1, app="bfs", nsrc=8, src_seed=2),
 }
 HEADLINE = "sssp-road-4096"
+TUNED = ROOT / "galoisgpu_b200" / "tuned_b200.json"
+
+
+def tuned_for(gft, name: str, spec: dict):
+    """(Tune, delta) from the committed autotuner results, else defaults."""
+    try:
+        t = json.loads(TUNED.read_text()).get(name)
+    except Exception:
+        t = None
+    delta = spec.get("delta")
+    if not t:
+        return None, delta, None
+    tune = gft.Tune(block_threads=t["block_threads"], blocks_per_sm=t["blocks_per_sm"], hub_degree=t["hub_degree"])
+    if spec["app"] == "sssp" and "delta" in t:
+        delta = t["delta"]
+    return tune, delta, {k: t[k] for k in ("block_threads", "blocks_per_sm", "hub_degree") if k in t}
 L2_BYTES = 126 * 2**20
 
 
@@ -204,15 +221,17 @@ def make_host_graph(gft, spec: dict):
 # ---------------------------------------------------------------------------
 # our arm
 # ---------------------------------------------------------------------------
-def run_queries(gft, eng, dg, spec, sources, out, stream):
+def run_queries(gft, eng, dg, spec, sources, out, stream, tune=None, delta=None, stats=None):
     app = spec["app"]
     kms = []
     for s in sources:
         if app == "sssp":
-            r = eng.sssp(dg, s, delta=spec["delta"], out=out, stream=stream)
+            r = eng.sssp(dg, s, delta=delta, out=out, stream=stream, tune=tune)
         else:
-            r = eng.bfs(dg, s, out=out, stream=stream)
+            r = eng.bfs(dg, s, out=out, stream=stream, tune=tune)
         kms.append(r["kernel_ms"])
+        if stats is not None:
+            stats.append({k: r[k] for k in ("levels", "iterations", "edges_scanned", "grid_blocks", "block_threads")})
     return kms
 
 
@@ -229,23 +248,25 @@ def bench_workload(gft, name: str, steps: int, warmup: int, d, dev: int, headlin
     eng = gft.Engine(dev)
     stream = torch.cuda.current_stream(dev)
     out = torch.empty(dg.nnodes, dtype=torch.int32, device=f"cuda:{dev}")
+    tune, delta, tune_desc = tuned_for(gft, name, spec)
 
     # Per-source reach statistics (E_r, V_r) from the first run of each source.
     reach = {}
+    qstats = []
     for s in sources:
-        run_queries(gft, eng, dg, spec, [s], out, stream)
+        run_queries(gft, eng, dg, spec, [s], out, stream, tune, delta, qstats)
         reach[s] = gft.reach_stats(dg, out, stream)
     step_src = [sources[i % len(sources)] for i in range(max(steps, len(sources)))]
     timed_src = step_src[:steps] if len(sources) <= steps else sources
     k = len(timed_src)
 
-    run_queries(gft, eng, dg, spec, [sources[i % len(sources)] for i in range(warmup)], out, stream)
+    run_queries(gft, eng, dg, spec, [sources[i % len(sources)] for i in range(warmup)], out, stream, tune, delta)
     clocks = ClockSampler(gpu_id_for(dev), str(dev)) if headline and d.rank == 0 else None
     d.barrier()
     torch.cuda.synchronize(dev)
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     ev0.record(stream)
-    kms = run_queries(gft, eng, dg, spec, timed_src, out, stream)
+    kms = run_queries(gft, eng, dg, spec, timed_src, out, stream, tune, delta)
     ev1.record(stream)
     torch.cuda.synchronize(dev)
     d.barrier()
@@ -265,11 +286,11 @@ def bench_workload(gft, name: str, steps: int, warmup: int, d, dev: int, headlin
     k_e2e = max(3, min(k, 10))
     e2e_src = [timed_src[i % len(timed_src)] for i in range(k_e2e)]
     for s in e2e_src[:2]:
-        (eng.sssp_host(dg, s, h_out, delta=spec["delta"]) if app == "sssp" else eng.bfs_host(dg, s, h_out))
+        (eng.sssp_host(dg, s, h_out, delta=delta, tune=tune) if app == "sssp" else eng.bfs_host(dg, s, h_out, tune=tune))
     d.barrier()
     t1 = time.perf_counter()
     for s in e2e_src:
-        (eng.sssp_host(dg, s, h_out, delta=spec["delta"]) if app == "sssp" else eng.bfs_host(dg, s, h_out))
+        (eng.sssp_host(dg, s, h_out, delta=delta, tune=tune) if app == "sssp" else eng.bfs_host(dg, s, h_out, tune=tune))
     e2e_s = d.max(time.perf_counter() - t1)
     e2e_value = d.world * sum(reach[s][1] for s in e2e_src) / (e2e_s * 1e9)
 
@@ -298,6 +319,9 @@ def bench_workload(gft, name: str, steps: int, warmup: int, d, dev: int, headlin
                      "kernel": kname, "traffic_source": traffic_src},
         "clocks": clk,
         "graph_bytes": (dg.nnodes + 1) * 4 + dg.nedges * (8 if dg.weighted else 4),
+        "tuning": tune_desc,
+        "delta": delta,
+        "query_stats": qstats[:4],
         "host": host,
         "out_last": out,
         "timed_src": timed_src,
@@ -365,6 +389,9 @@ def our_arm(args) -> int:
             "parallelism": f"replicas x{d.world}",
             "kernel_ms_mean": res["kernel_ms_mean"],
             "gteps_hmean_kernel": res["gteps_hmean_kernel"],
+            "delta": res["delta"],
+            "tuning": res["tuning"] or "engine defaults",
+            "query_stats": res["query_stats"],
         },
         "e2e": res["e2e"],
         "gpu_launches": res["k"],
@@ -398,6 +425,7 @@ def our_arm(args) -> int:
                     cb2, par2 = cpu_baseline(orc, WORKLOADS[sname], r2["host"], s2, r2["reach"],
                                              _rerun(gft, dg2, WORKLOADS[sname], s2, dev))
                     sec[sname] = {
+                        "tuning": r2["tuning"], "query_stats": r2["query_stats"][:2],
                         "value": r2["value"], "unit": "GTEPS", "gteps_hmean_kernel": r2["gteps_hmean_kernel"],
                         "kernel_ms_mean": r2["kernel_ms_mean"], "queries": r2["k"], "nodes": r2["nodes"],
                         "edges": r2["edges"], "E_r_per_query": r2["e_r_per_query"], "e2e": r2["e2e"],
