@@ -828,3 +828,129 @@ gft_status gft_reach_stats(const gft_graph *g, const int32_t *d_val, void *strea
 
 }  // extern "C"
 
+// ---------------------------------------------------------------------------
+// Allocation-free BFS (gft_bfs_noalloc)
+//
+// For callers that must not allocate device memory themselves or through
+// the library: code running while another component owns the device's
+// memory (a caching allocator that has reserved the free memory, or a
+// framework that forbids allocations outside its own pool), and hot paths
+// where cudaMalloc / cudaFree are not allowed because of their implicit
+// synchronisation.  The traversal scratch (control block, two frontier
+// queues, visited bitmap, hub list) lives in one file-scope device array of
+// fixed size, sized for graphs of up to kNoAllocMaxNodes vertices; every GPU
+// that loads libgft holds it until the process exits.
+//
+// The array's name is only a host-side stand-in in host code, so its device
+// address is looked up once per device with cudaGetSymbolAddress (with that
+// device current) on the first call for that device; make that first call
+// before any stream capture.  All calls share the array: the control block
+// is cleared on the call's stream before the launch, and calls whose work
+// overlaps on the GPU race on the scratch, so serialise them (one stream, or
+// events between streams).
+// ---------------------------------------------------------------------------
+namespace gft {
+namespace {
+
+constexpr uint32_t kNoAllocMaxNodes = 1u << 20;  // 1,048,576 vertices
+constexpr int kNoAllocBlock = 512;
+
+constexpr size_t na_align(size_t x) { return (x + 255) & ~(size_t)255; }
+constexpr size_t kNoAllocCtlBytes = na_align(sizeof(TraversalCtl));
+constexpr size_t kNoAllocQueueBytes = na_align((size_t)kNoAllocMaxNodes * 4);
+constexpr size_t kNoAllocBitmapBytes = na_align((size_t)(kNoAllocMaxNodes / 32) * 4);
+constexpr size_t kNoAllocHubBytes = na_align((size_t)kNoAllocMaxNodes * 8);
+constexpr size_t kNoAllocBytes = kNoAllocCtlBytes + 2 * kNoAllocQueueBytes + kNoAllocBitmapBytes + kNoAllocHubBytes;
+
+__device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
+
+std::mutex g_noalloc_mu;
+void *g_noalloc_addr[256];
+
+gft_status noalloc_scratch(int device, char **out)
+{
+    if (device < 0 || device >= 256) return fail(GFT_ERR_INVALID_ARG, "gft_bfs_noalloc: device %d", device);
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (!g_noalloc_addr[device]) {
+        void *p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess || !p)
+            return fail(GFT_ERR_CUDA, "gft_bfs_noalloc: cudaGetSymbolAddress failed on device %d: %s", device,
+                        cudaGetErrorString(e));
+        g_noalloc_addr[device] = p;
+    }
+    *out = static_cast<char *>(g_noalloc_addr[device]);
+    return GFT_OK;
+}
+
+}  // namespace
+}  // namespace gft
+
+extern "C" gft_status gft_bfs_noalloc(const gft_graph *g, uint32_t src, int32_t *d_level, uint32_t *d_parent,
+                                      const gft_tuning *tune, void *stream_, gft_stats *stats)
+{
+    using namespace gft;
+    if (!g || !d_level) return fail(GFT_ERR_INVALID_ARG, "gft_bfs_noalloc: null argument");
+    const DeviceGraph &G = g->g;
+    if (G.nnodes > kNoAllocMaxNodes)
+        return fail(GFT_ERR_INVALID_ARG, "gft_bfs_noalloc: %u vertices exceed the fixed scratch limit of %u",
+                    G.nnodes, kNoAllocMaxNodes);
+    if (src >= G.nnodes)
+        return fail(GFT_ERR_INVALID_ARG, "gft_bfs_noalloc: source %u out of range (nnodes %u)", src, G.nnodes);
+    uint32_t hub = (tune && tune->hub_degree) ? std::max<uint32_t>(tune->hub_degree, 32) : 4096;
+    uint32_t timeout_ms = (tune && tune->timeout_ms) ? tune->timeout_ms : 20000;
+    cudaStream_t stream = (cudaStream_t)stream_;
+    GFT_CUDA_TRY(cudaSetDevice(G.device));
+    char *base = nullptr;
+    GFT_TRY(noalloc_scratch(G.device, &base));
+
+    const void *kern = (const void *)dev::bfs_persistent<kNoAllocBlock>;
+    int sms = 0, occ = 0;
+    GFT_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, G.device));
+    GFT_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kNoAllocBlock, 0));
+    if (occ <= 0) return fail(GFT_ERR_NOT_SUPPORTED, "gft_bfs_noalloc: kernel cannot be resident");
+    const int blocks = sms * std::min(occ, 2);
+
+    dev::TravParams p{};
+    p.row_start = G.row_start;
+    p.edge_dst = G.edge_dst;
+    p.edge_data = nullptr;
+    p.nnodes = G.nnodes;
+    p.src = src;
+    p.out = d_level;
+    p.parent = d_parent;
+    p.ctl = reinterpret_cast<TraversalCtl *>(base);
+    p.q[0] = reinterpret_cast<uint32_t *>(base + kNoAllocCtlBytes);
+    p.q[1] = reinterpret_cast<uint32_t *>(base + kNoAllocCtlBytes + kNoAllocQueueBytes);
+    p.visited = reinterpret_cast<uint32_t *>(base + kNoAllocCtlBytes + 2 * kNoAllocQueueBytes);
+    p.hubs = reinterpret_cast<uint2 *>(base + kNoAllocCtlBytes + 2 * kNoAllocQueueBytes + kNoAllocBitmapBytes);
+    p.hub_cap = (uint32_t)std::min<uint64_t>(G.nnodes, (uint64_t)G.nedges / hub + 1);
+    p.hub_degree = hub;
+    p.qcap = G.nnodes;
+    p.timeout_ns = (unsigned long long)timeout_ms * 1000000ull;
+    p.skip_block = -1;
+    p.vec_ok = ((uintptr_t)G.edge_dst % 16 == 0);
+
+    // The control block must start at zero for every call.
+    GFT_CUDA_TRY(cudaMemsetAsync(p.ctl, 0, sizeof(TraversalCtl), stream));
+    void *args[] = {&p};
+    GFT_CUDA_TRY(cudaLaunchCooperativeKernel(kern, dim3(blocks), dim3(kNoAllocBlock), args, 0, stream));
+    TraversalCtl h;
+    const size_t cold = offsetof(TraversalCtl, error);
+    GFT_CUDA_TRY(cudaMemcpyAsync(reinterpret_cast<char *>(&h) + cold, reinterpret_cast<char *>(p.ctl) + cold,
+                                 sizeof(TraversalCtl) - cold, cudaMemcpyDeviceToHost, stream));
+    GFT_CUDA_TRY(cudaStreamSynchronize(stream));
+    if (h.error)
+        return fail((gft_status)h.error, "gft_bfs_noalloc: device reported %s (site %u)",
+                    gft_status_string((gft_status)h.error), h.error_where);
+    if (stats) {
+        memset(stats, 0, sizeof *stats);
+        stats->levels = h.levels;
+        stats->iterations = h.iterations;
+        stats->edges_scanned = h.edges;
+        stats->vertices_reached = h.reached + 1;
+        stats->grid_blocks = blocks;
+        stats->block_threads = kNoAllocBlock;
+    }
+    return GFT_OK;
+}

@@ -207,6 +207,26 @@ GFT_API gft_status gft_bfs_host(gft_engine *e, const gft_graph *g, uint32_t src,
 GFT_API gft_status gft_sssp_host(gft_engine *e, const gft_graph *g, uint32_t src, int32_t delta, int32_t *h_dist,
                          uint32_t *h_parent, const gft_tuning *tune, void *stream, gft_stats *stats);
 
+/* Allocation-free BFS.  No counterpart in the reference: gg_main allocates
+ * its worklists on every call (apps/bfs/kernel.cu:389, rt/include/worklist.h:
+ * 73-118).  For callers that cannot call cudaMalloc -- code running while
+ * another component owns the device memory, or paths where an allocation's
+ * implicit synchronisation is not allowed -- this variant neither allocates
+ * nor frees anything: no engine, no cudaMalloc/cudaFree, no allocating
+ * library routine.  Its scratch is one fixed file-scope device array
+ * (about 16.2 MB, held by every GPU that loads libgft until exit), so the
+ * graph may have at most 1,048,576 vertices; larger graphs are rejected with
+ * GFT_ERR_INVALID_ARG.  The caller passes the graph and the output buffers
+ * (d_level, optional d_parent) as for gft_bfs; results are identical.
+ * The first call on a device looks up the array's device address
+ * (cudaGetSymbolAddress with that device current); make that first call
+ * before any stream capture.  Every call reuses the same array (the control
+ * block is cleared on `stream` before each launch), so calls whose work
+ * overlaps on the GPU race: serialise them.  Waits for `stream`; stats as
+ * for gft_bfs except kernel_ms (0: no events are created). */
+GFT_API gft_status gft_bfs_noalloc(const gft_graph *g, uint32_t src, int32_t *d_level, uint32_t *d_parent,
+                                   const gft_tuning *tune, void *stream, gft_stats *stats);
+
 /* Reach statistics of a result already on the device: V_r (vertices with a
  * finite value) and E_r (sum of their out-degrees, the edges a top-down
  * traversal must scan).  Waits for `stream`. */
