@@ -6,6 +6,7 @@ ABI of include/gft.h); this package is the Python host side.
 """
 
 from .graph import (  # noqa: F401
+    Batch,
     DEFAULT_DELTA,
     GFT_NO_PARENT,
     INF,

@@ -72,6 +72,9 @@ class Tuning(C.Structure):
         ("hub_degree", C.c_uint32),
         ("timeout_ms", C.c_uint32),
         ("test_skip_block", C.c_int32),
+        ("max_blocks", C.c_uint32),
+        ("group_blocks", C.c_uint32),
+        ("group_min_nodes", C.c_uint32),
     ]
 
 
@@ -89,6 +92,65 @@ class GenParams(C.Structure):
         ("shortcut_ppm", C.c_uint32),
         ("max_weight", C.c_uint32),
         ("seed", C.c_uint64),
+    ]
+
+
+class Query(C.Structure):
+    _fields_ = [
+        ("graph", C.c_void_p),
+        ("app", C.c_uint32),
+        ("src", C.c_uint32),
+        ("delta", C.c_int32),
+        ("d_out", C.c_void_p),
+        ("d_parent", C.c_void_p),
+        ("status", C.c_int),
+        ("levels", C.c_uint32),
+        ("iterations", C.c_uint32),
+        ("edges_scanned", C.c_uint64),
+        ("device_ms", C.c_float),
+    ]
+
+
+class BatchStats(C.Structure):
+    _fields_ = [
+        ("queries", C.c_uint32),
+        ("launch_ms", C.c_float),
+        ("busy_ms", C.c_float),
+        ("edges_scanned", C.c_uint64),
+        ("grid_blocks", C.c_uint32),
+        ("block_threads", C.c_uint32),
+        ("scratch_bytes", C.c_size_t),
+    ]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+class ServeConfig(C.Structure):
+    _fields_ = [
+        ("lanes", C.c_uint32),
+        ("max_batch", C.c_uint32),
+        ("lane_arena_bytes", C.c_size_t),
+        ("block_threads", C.c_uint32),
+        ("hub_degree", C.c_uint32),
+        ("lane_blocks", C.c_uint32),
+        ("group_blocks", C.c_uint32),
+        ("group_min_nodes", C.c_uint32),
+        ("sparse_degree", C.c_uint32),
+        ("queue_capacity", C.c_uint32),
+    ]
+
+
+class Completion(C.Structure):
+    _fields_ = [
+        ("ticket", C.c_uint64),
+        ("status", C.c_int),
+        ("latency_ms", C.c_double),
+        ("queue_ms", C.c_double),
+        ("lane", C.c_uint32),
+        ("batch_size", C.c_uint32),
+        ("levels", C.c_uint32),
+        ("edges_scanned", C.c_uint64),
     ]
 
 
@@ -114,6 +176,7 @@ _SIGS: dict[str, tuple] = {
     "gft_graph_info": (C.c_int, [_P, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.POINTER(C.c_int)]),
     "gft_graph_arrays": (C.c_int, [_P, C.POINTER(_P), C.POINTER(_P), C.POINTER(_P)]),
     "gft_graph_download": (C.c_int, [_P, C.POINTER(Csr)]),
+    "gft_graph_pick_sources": (C.c_int, [_P, C.c_uint64, C.c_uint32, C.POINTER(C.c_uint32)]),
     "gft_graph_free": (None, [_P]),
     "gft_engine_create": (C.c_int, [C.c_int, C.POINTER(_P)]),
     "gft_engine_destroy": (None, [_P]),
@@ -125,6 +188,21 @@ _SIGS: dict[str, tuple] = {
     "gft_reach_stats": (C.c_int, [_P, _P, _P, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
     "gft_bfs_noalloc": (C.c_int, [_P, C.c_uint32, _P, _P, C.POINTER(Tuning), _P, C.POINTER(Stats)]),
     "gft_write_output": (C.c_int, [C.c_char_p, C.c_uint32, _P]),
+    "gft_batch_create": (C.c_int, [_P, C.POINTER(Query), C.c_uint32, C.POINTER(Tuning), C.POINTER(_P)]),
+    "gft_batch_set_source": (C.c_int, [_P, C.c_uint32, C.c_uint32]),
+    "gft_batch_submit": (C.c_int, [_P, _P]),
+    "gft_batch_wait": (C.c_int, [_P, C.POINTER(Query), C.POINTER(BatchStats)]),
+    "gft_batch_destroy": (None, [_P]),
+    "gft_msbfs_plane_bytes": (C.c_size_t, [C.c_uint32, C.c_uint32]),
+    "gft_msbfs": (C.c_int, [_P, _P, C.POINTER(C.c_uint32), C.c_uint32, _P, C.c_uint32, C.c_uint32, _P,
+                            C.POINTER(Stats)]),
+    "gft_msbfs_levels": (C.c_int, [_P, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, _P, _P]),
+    "gft_serve_config_default": (C.c_int, [C.POINTER(ServeConfig)]),
+    "gft_serve_open": (C.c_int, [_P, C.POINTER(ServeConfig), C.POINTER(_P)]),
+    "gft_serve_enqueue": (C.c_int, [_P, C.POINTER(Query), C.POINTER(C.c_uint64)]),
+    "gft_serve_poll": (C.c_int, [_P, C.POINTER(Completion), C.c_uint32, C.POINTER(C.c_uint32), C.c_uint32]),
+    "gft_serve_stats": (C.c_int, [_P, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
+    "gft_serve_close": (C.c_int, [_P]),
 }
 
 _lock = threading.Lock()

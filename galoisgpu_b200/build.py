@@ -37,8 +37,11 @@ LIB_SOURCES = [
     "engine.cu",
     "traversal.cu",
     "gen_device.cu",
+    "batch.cu",
+    "msbfs.cu",
+    "serve.cpp",
 ]
-HEADERS = ["gft_internal.h", "gen_common.h", "traverse.cuh"]
+HEADERS = ["gft_internal.h", "gen_common.h", "traverse.cuh", "frontier.cuh"]
 CLI_SOURCE = "cli_main.cpp"
 
 NVCC_FLAGS = [

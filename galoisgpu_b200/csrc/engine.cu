@@ -229,6 +229,15 @@ gft_status gft_graph_download(const gft_graph *g, gft_csr *out)
     return GFT_OK;
 }
 
+gft_status gft_graph_pick_sources(const gft_graph *g, uint64_t seed, uint32_t k, uint32_t *out_sources)
+{
+    if (!g || (k && !out_sources)) return fail(GFT_ERR_INVALID_ARG, "gft_graph_pick_sources: null argument");
+    std::vector<uint32_t> rs((size_t)g->g.nnodes + 1);
+    GFT_CUDA_TRY(cudaSetDevice(g->g.device));
+    GFT_CUDA_TRY(cudaMemcpy(rs.data(), g->g.row_start, rs.size() * 4, cudaMemcpyDeviceToHost));
+    return pick_sources_rs(g->g.nnodes, rs.data(), seed, k, out_sources);
+}
+
 void gft_graph_free(gft_graph *g)
 {
     if (!g) return;

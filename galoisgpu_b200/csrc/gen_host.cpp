@@ -121,6 +121,25 @@ static gft_status build_symmetric(uint32_t nnodes, uint64_t npairs, Get get, uin
     return GFT_OK;
 }
 
+// Draws k distinct vertices of out-degree > 0: draw i of the source stream,
+// modulo nnodes, skipping repeats and isolated vertices.
+gft_status pick_sources_rs(uint32_t nnodes, const uint32_t *row_start, uint64_t seed, uint32_t k, uint32_t *out)
+{
+    if (nnodes == 0 && k) return fail(GFT_ERR_INVALID_ARG, "pick_sources: empty graph");
+    uint64_t key = stream_key(seed, kStreamSource);
+    std::unordered_set<uint32_t> seen;
+    uint32_t got = 0;
+    uint64_t limit = 64ull * nnodes + (1u << 20);
+    for (uint64_t i = 0; got < k && i < limit; i++) {
+        uint32_t v = (uint32_t)(draw(key, i) % nnodes);
+        if (row_start[v + 1] == row_start[v] || seen.count(v)) continue;
+        seen.insert(v);
+        out[got++] = v;
+    }
+    if (got < k) return fail(GFT_ERR_INVALID_ARG, "pick_sources: only %u of %u sources found", got, k);
+    return GFT_OK;
+}
+
 }  // namespace gft
 
 using namespace gft;
@@ -193,18 +212,7 @@ gft_status gft_gen_rmat(uint32_t scale, uint32_t edge_factor, uint32_t a_q32, ui
 gft_status gft_pick_sources(const gft_csr *g, uint64_t seed, uint32_t k, uint32_t *out_sources)
 {
     if (!g || !g->row_start || (k && !out_sources)) return fail(GFT_ERR_INVALID_ARG, "gft_pick_sources: null argument");
-    uint64_t key = stream_key(seed, kStreamSource);
-    std::unordered_set<uint32_t> seen;
-    uint32_t got = 0;
-    uint64_t limit = 64ull * g->nnodes + (1u << 20);
-    for (uint64_t i = 0; got < k && i < limit; i++) {
-        uint32_t v = (uint32_t)(draw(key, i) % g->nnodes);
-        if (g->row_start[v + 1] == g->row_start[v] || seen.count(v)) continue;
-        seen.insert(v);
-        out_sources[got++] = v;
-    }
-    if (got < k) return fail(GFT_ERR_INVALID_ARG, "gft_pick_sources: only %u of %u sources found", got, k);
-    return GFT_OK;
+    return gft::pick_sources_rs(g->nnodes, g->row_start, seed, k, out_sources);
 }
 
 }  // extern "C"

@@ -72,6 +72,7 @@ struct TraversalCtl {
     CtlLine hub_claim[3];  // hub chunk cursor per iteration slot (u32)
     CtlLine far_len[3];    // SSSP far pile length per phase slot (u32)
     CtlLine far_min[3];    // SSSP least distance sent to the far pile per phase slot (u32)
+    CtlLine job;           // batch kernel: job claimed by a CTA group (u32)
     // Cold fields, written once per launch.
     unsigned error;        // gft_status recorded by the device (0 = none)
     unsigned error_where;  // barrier episode or queue index of the failure
@@ -85,6 +86,25 @@ struct TraversalCtl {
 };
 
 __host__ __device__ inline unsigned *u32_of(CtlLine &l) { return reinterpret_cast<unsigned *>(&l.v); }
+
+// One query of a batched / served launch (device job table entry).  The
+// CTA that runs the job writes the result fields.
+struct BatchJob {
+    const uint32_t *row_start;
+    const uint32_t *edge_dst;
+    const int32_t *edge_data;
+    int32_t *out;
+    uint32_t *parent;
+    unsigned long long scratch;  // byte offset of this job's scratch
+    uint32_t nnodes, nedges, src, delta;
+    uint32_t app;  // 0 BFS, 1 SSSP
+    uint32_t hub_cap;
+    uint32_t vec_ok;
+    uint32_t pad;
+    uint32_t status, error_where, levels, iterations;
+    unsigned long long edges;
+    unsigned long long t_start, t_end;  // %globaltimer, ns
+};
 
 struct LaunchShape {
     int block_threads = 512;
@@ -120,4 +140,15 @@ gft_status check_engine_graph(gft_engine *e, const gft_graph *g);
 gft_status run_traversal(bool is_sssp, gft_engine *e, const gft_graph *g, uint32_t src, int32_t delta, int32_t *d_out,
                          uint32_t *d_parent, const gft_tuning *tune, cudaStream_t stream, gft_stats *stats);
 gft_status reach_stats(const gft_graph *g, const int32_t *d_val, cudaStream_t stream, uint64_t *v_r, uint64_t *e_r);
+gft_status pick_sources_rs(uint32_t nnodes, const uint32_t *row_start, uint64_t seed, uint32_t k, uint32_t *out);
+// CTA-mode batch kernel plumbing shared by gft_batch_* and the server.
+// jobs[0, nbig) run on groups of `group` CTAs (cooperative launch, one
+// zeroed TraversalCtl per group in d_gctl), the rest on one CTA each;
+// d_cursors holds 2 counters.
+gft_status launch_batch_jobs(const BatchJob *d_jobs, unsigned njobs, unsigned nbig, unsigned group,
+                             unsigned *d_cursors, char *d_scratch, uint32_t hub_degree, TraversalCtl *d_gctl,
+                             int block, int blocks, cudaStream_t stream);
+int batch_occupancy(int block);
+void fill_batch_job(BatchJob &j, const gft_query &x, uint32_t hub_degree);
+size_t batch_job_scratch(uint32_t app, uint32_t nnodes, uint32_t hub_cap);
 }  // namespace gft

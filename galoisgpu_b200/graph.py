@@ -27,7 +27,7 @@ from pathlib import Path
 import numpy as np
 
 from . import _lib
-from ._lib import GFT_INF, GFT_NO_PARENT, Csr, GenParams, Stats, Tuning, check, load
+from ._lib import GFT_INF, GFT_NO_PARENT, BatchStats, Csr, GenParams, Query, Stats, Tuning, check, load
 
 INF = GFT_INF  # apps/bfs/kernel.cu:16, apps/sssp/kernel.cu:18
 DEFAULT_DELTA = 10000  # apps/sssp/support.cu:56
@@ -214,6 +214,12 @@ class DeviceGraph:
         check(load().gft_graph_arrays(self.handle, C.byref(rs), C.byref(dst), C.byref(w)))
         return rs.value or 0, dst.value or 0, w.value or 0
 
+    def pick_sources(self, seed: int, k: int) -> list[int]:
+        """Same draw as CSRGraph.pick_sources, reading only row_start."""
+        out = (C.c_uint32 * k)()
+        check(load().gft_graph_pick_sources(self.handle, seed, k, out))
+        return list(out)
+
     def download(self) -> CSRGraph:
         csr = Csr()
         check(load().gft_graph_download(self.handle, C.byref(csr)))
@@ -240,9 +246,13 @@ class Tune:
     hub_degree: int = 0
     timeout_ms: int = 0
     test_skip_block: int = -1
+    max_blocks: int = 0
+    group_blocks: int = 0
+    group_min_nodes: int = 0
 
     def c(self) -> Tuning:
-        return Tuning(self.block_threads, self.blocks_per_sm, self.hub_degree, self.timeout_ms, self.test_skip_block)
+        return Tuning(self.block_threads, self.blocks_per_sm, self.hub_degree, self.timeout_ms, self.test_skip_block,
+                      self.max_blocks, self.group_blocks, self.group_min_nodes)
 
 
 class Engine:
@@ -311,6 +321,36 @@ class Engine:
         )
         return {"out": out, "parent": parent, **st.as_dict()}
 
+    def msbfs(self, graph: DeviceGraph, sources: list[int], max_levels: int = 32, symmetric: bool = False,
+              planes=None, stream=None) -> dict:
+        """Multi-source BFS of up to 256 sources; returns the frontier planes
+        (a uint32 device tensor) and stats.  levels(i) gives source i's
+        int32 levels."""
+        import torch
+
+        k = len(sources)
+        words = (k + 31) // 32
+        if planes is None:
+            planes = torch.empty(max_levels * graph.nnodes * words, dtype=torch.int32,
+                                 device=f"cuda:{graph.device}")
+        src = (C.c_uint32 * k)(*sources)
+        st = Stats()
+        dev = torch.device("cuda", graph.device)
+        s = stream if stream is not None else torch.cuda.current_stream(dev)
+        check(load().gft_msbfs(self._h, graph.handle, src, k, C.c_void_p(planes.data_ptr()), max_levels,
+                               1 if symmetric else 0, _stream_ptr(s), C.byref(st)))
+        res = {"planes": planes, "k": k, **st.as_dict()}
+
+        def levels(i: int, out=None):
+            if out is None:
+                out = torch.empty(graph.nnodes, dtype=torch.int32, device=dev)
+            check(load().gft_msbfs_levels(C.c_void_p(planes.data_ptr()), graph.nnodes, k, st.levels, i,
+                                          C.c_void_p(out.data_ptr()), _stream_ptr(s)))
+            return out
+
+        res["levels_of"] = levels
+        return res
+
     def bfs_host(self, graph: DeviceGraph, start_node: int, out: np.ndarray, parent: np.ndarray | None = None,
                  tune: Tune | None = None, stream=None) -> dict:
         """End-to-end query with host result buffers (int32 / uint32 numpy)."""
@@ -337,6 +377,74 @@ class Engine:
         return st.as_dict()
 
 
+class Batch:
+    """Many queries in one persistent launch, replayed as a CUDA graph
+    (gft_batch_*).  `queries` are dicts with keys graph, app ('bfs' or
+    'sssp'), src, optional delta, out (int32 device tensor, allocated when
+    absent) and parent (BFS only)."""
+
+    def __init__(self, engine: "Engine", queries: list[dict], tune: Tune | None = None):
+        import torch
+
+        self.engine = engine
+        self.queries = []
+        self._keep = []
+        arr = (Query * len(queries))()
+        for i, q in enumerate(queries):
+            g: DeviceGraph = q["graph"]
+            out = q.get("out")
+            if out is None:
+                out = torch.empty(g.nnodes, dtype=torch.int32, device=f"cuda:{g.device}")
+            par = q.get("parent")
+            arr[i].graph = g.handle
+            arr[i].app = 1 if q["app"] == "sssp" else 0
+            arr[i].src = q["src"]
+            arr[i].delta = q.get("delta", DEFAULT_DELTA) if q["app"] == "sssp" else 0
+            arr[i].d_out = out.data_ptr()
+            arr[i].d_parent = par.data_ptr() if par is not None else None
+            self.queries.append({**q, "out": out, "parent": par})
+            self._keep += [g, out, par]
+        self._arr = arr
+        h = C.c_void_p()
+        check(load().gft_batch_create(engine._h, arr, len(queries), engine._tune(tune), C.byref(h)))
+        self._h = h
+
+    def set_source(self, i: int, src: int) -> None:
+        check(load().gft_batch_set_source(self._h, i, src))
+        self.queries[i]["src"] = src
+
+    def submit(self, stream=None) -> None:
+        import torch
+
+        dev = self.queries[0]["graph"].device
+        s = stream if stream is not None else torch.cuda.current_stream(dev)
+        check(load().gft_batch_submit(self._h, _stream_ptr(s)))
+
+    def wait(self) -> dict:
+        st = BatchStats()
+        check(load().gft_batch_wait(self._h, self._arr, C.byref(st)))
+        for i, q in enumerate(self.queries):
+            a = self._arr[i]
+            q.update(status=a.status, levels=a.levels, iterations=a.iterations, edges_scanned=a.edges_scanned,
+                     device_ms=a.device_ms)
+        return st.as_dict()
+
+    def run(self, stream=None) -> dict:
+        self.submit(stream)
+        return self.wait()
+
+    def close(self) -> None:
+        if getattr(self, "_h", None) is not None:
+            load().gft_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 def reach_stats(graph: DeviceGraph, values, stream=None) -> tuple[int, int]:
     """(V_r, E_r) of a device result tensor."""
     vr, er = C.c_uint64(), C.c_uint64()
@@ -352,6 +460,7 @@ def output(path: str | Path, values: np.ndarray) -> None:
 
 
 __all__ = [
+    "Batch",
     "CSRGraph",
     "DeviceGraph",
     "Engine",

@@ -87,6 +87,11 @@ typedef struct gft_tuning {
     uint32_t hub_degree;      /* degree at which a vertex is split across the grid  */
     uint32_t timeout_ms;      /* bound on every device-side wait                    */
     int32_t test_skip_block;  /* test hook: CTA that never arrives (-1 = none)      */
+    uint32_t max_blocks;      /* cap on the persistent grid (0 = no cap)            */
+    uint32_t group_blocks;    /* batches: CTAs that share one large query (0 = 8)   */
+    uint32_t group_min_nodes; /* batches: queries on graphs with at least this many
+                                 vertices run on a CTA group (0 = 262144; set it
+                                 above every graph to run each query on one CTA) */
 } gft_tuning;
 
 /* ---------------------------------------------------------------------------
@@ -162,6 +167,8 @@ GFT_API gft_status gft_graph_info(const gft_graph *g, uint32_t *nnodes, uint32_t
 /* Device pointers of a graph (any may be NULL). */
 GFT_API gft_status gft_graph_arrays(const gft_graph *g, const uint32_t **d_row_start, const uint32_t **d_edge_dst,
                             const int32_t **d_edge_data);
+/* gft_pick_sources for a device graph (reads only its row_start). */
+GFT_API gft_status gft_graph_pick_sources(const gft_graph *g, uint64_t seed, uint32_t k, uint32_t *out_sources);
 /* Copies a device graph back to a host CSR (arrays malloc'd). */
 GFT_API gft_status gft_graph_download(const gft_graph *g, gft_csr *out);
 GFT_API void gft_graph_free(gft_graph *g);
@@ -226,6 +233,130 @@ GFT_API gft_status gft_sssp_host(gft_engine *e, const gft_graph *g, uint32_t src
  * for gft_bfs except kernel_ms (0: no events are created). */
 GFT_API gft_status gft_bfs_noalloc(const gft_graph *g, uint32_t src, int32_t *d_level, uint32_t *d_parent,
                                    const gft_tuning *tune, void *stream, gft_stats *stats);
+
+/* ---------------------------------------------------------------------------
+ * Batched queries (no counterpart in the reference, which runs one query per
+ * process: skelapp/skel.cu:139-151).  Many BFS / SSSP queries, on one or many
+ * resident graphs, run in one persistent launch: each query runs on one CTA
+ * (control block in shared memory, block-level barriers), the largest
+ * queries first.  The launch (job-table upload, cursor reset, kernel) is
+ * captured once as a CUDA graph by gft_batch_create and replayed by every
+ * gft_batch_submit.  Results are identical to gft_bfs / gft_sssp.
+ * ------------------------------------------------------------------------- */
+#define GFT_APP_BFS 0u
+#define GFT_APP_SSSP 1u
+
+typedef struct gft_query {
+    const gft_graph *graph;
+    uint32_t app;        /* GFT_APP_BFS or GFT_APP_SSSP                        */
+    uint32_t src;
+    int32_t delta;       /* SSSP bucket width (> 0)                            */
+    int32_t *d_out;      /* device, nnodes int32: levels / distances           */
+    uint32_t *d_parent;  /* device, nnodes, or NULL (BFS only in batches)      */
+    /* filled by gft_batch_wait */
+    gft_status status;
+    uint32_t levels, iterations;
+    uint64_t edges_scanned;
+    float device_ms;     /* time the query occupied its CTA                    */
+} gft_query;
+
+typedef struct gft_batch_stats {
+    uint32_t queries;
+    float launch_ms;        /* device time of the whole launch (events)      */
+    float busy_ms;          /* first query start to last query end (device)  */
+    uint64_t edges_scanned;
+    uint32_t grid_blocks, block_threads;
+    size_t scratch_bytes;   /* device scratch held by the batch               */
+} gft_batch_stats;
+
+typedef struct gft_batch gft_batch;
+
+/* Validates the n queries, allocates the batch's scratch (per query: 2 or 6
+ * x nnodes x 4 bytes plus its hub list), uploads nothing yet and captures the
+ * launch.  tune: block_threads (256/512/1024), blocks_per_sm, hub_degree. */
+GFT_API gft_status gft_batch_create(gft_engine *e, const gft_query *q, uint32_t n, const gft_tuning *tune,
+                                    gft_batch **out);
+/* Changes query `query`'s source for the next submit (no re-capture). */
+GFT_API gft_status gft_batch_set_source(gft_batch *b, uint32_t query, uint32_t src);
+/* Replays the captured launch on `stream` (asynchronous). */
+GFT_API gft_status gft_batch_submit(gft_batch *b, void *stream);
+/* Waits for the last submit and fills each query's status and statistics
+ * (q may be NULL); returns the first failing query's status, if any. */
+GFT_API gft_status gft_batch_wait(gft_batch *b, gft_query *q, gft_batch_stats *stats);
+GFT_API void gft_batch_destroy(gft_batch *b);
+
+/* ---------------------------------------------------------------------------
+ * Serving (no counterpart in the reference, which runs one query per
+ * process).  A request loop over resident graphs with continuous batching.
+ * The device's resident CTAs are split into `lanes` of `lane_blocks` CTAs
+ * (default: one lane per group of `group_blocks` CTAs), each with its own
+ * stream and scratch arena, so their launches overlap on the device.  In
+ * arrival order, a heavy request (a graph of at least `group_min_nodes`
+ * vertices; with sparse_degree > 0, BFS on a graph of lower average degree
+ * counts as light) gets a free lane to itself and runs on its CTA group;
+ * a run of light requests shares one launch, one CTA each.  A request that
+ * arrives while others run starts as soon as a lane and arena space are
+ * free, and a long request never holds up a launch of short ones.  A
+ * request is taken only when its scratch fits in the lane's arena
+ * (`lane_arena_bytes`); one that could never fit is refused at enqueue with
+ * GFT_ERR_OOM, and a full queue returns GFT_ERR_BUSY.  The caller owns each
+ * request's output buffer (d_out) until its completion is polled.
+ * ------------------------------------------------------------------------- */
+typedef struct gft_serve_config {
+    uint32_t lanes;             /* streams (0 = resident CTAs / lane_blocks)     */
+    uint32_t max_batch;         /* light requests per launch (default 256)       */
+    size_t lane_arena_bytes;    /* scratch arena per lane (default 768 MiB)      */
+    uint32_t block_threads;     /* CTA size (default 512)                        */
+    uint32_t hub_degree;        /* default 256                                   */
+    uint32_t lane_blocks;       /* CTAs per lane (0 = group_blocks)              */
+    uint32_t group_blocks;      /* CTAs per heavy request (default 16)           */
+    uint32_t group_min_nodes;   /* default 2^18                                  */
+    uint32_t sparse_degree;     /* default 0 (no exception)                      */
+    uint32_t queue_capacity;    /* requests admitted but not completed           */
+} gft_serve_config;
+
+typedef struct gft_completion {
+    uint64_t ticket;
+    gft_status status;
+    double latency_ms;      /* enqueue -> completion observed                 */
+    double queue_ms;        /* enqueue -> launch                              */
+    uint32_t lane;          /* lane (1-based) that ran the request             */
+    uint32_t batch_size;    /* requests in the same launch                    */
+    uint32_t levels;
+    uint64_t edges_scanned;
+} gft_completion;
+
+typedef struct gft_server gft_server;
+
+GFT_API gft_status gft_serve_config_default(gft_serve_config *cfg);
+GFT_API gft_status gft_serve_open(gft_engine *e, const gft_serve_config *cfg, gft_server **out);
+/* Non-blocking; *ticket identifies the request's completion. */
+GFT_API gft_status gft_serve_enqueue(gft_server *s, const gft_query *q, uint64_t *ticket);
+/* Up to `max` completions; waits up to wait_us for the first one. */
+GFT_API gft_status gft_serve_poll(gft_server *s, gft_completion *out, uint32_t max, uint32_t *n, uint32_t wait_us);
+GFT_API gft_status gft_serve_stats(gft_server *s, uint64_t *in_flight, uint64_t *batches, uint64_t *queries);
+/* Finishes the admitted requests, then releases the server. */
+GFT_API gft_status gft_serve_close(gft_server *s);
+
+/* ---------------------------------------------------------------------------
+ * Multi-source BFS (no counterpart in the reference, which runs one source
+ * per process).  k <= 256 BFS queries on one graph in one launch with
+ * per-vertex bitsets (one bit per source).  The result is a stack of
+ * frontier planes in caller memory: d_planes holds max_levels planes of
+ * gft_msbfs_plane_bytes(nnodes, k) bytes each; plane L, vertex v, bit i is
+ * set iff source i reaches v at level L.  stats->levels = planes used;
+ * GFT_ERR_OVERFLOW if the traversal needs more than max_levels.
+ * gft_msbfs_levels writes source i's int32 levels (as gft_bfs would) from
+ * the planes.  flags: GFT_MSBFS_SYMMETRIC allows bottom-up levels (the
+ * graph's out-edges must also be its in-edges); without it every level is
+ * top-down.
+ * ------------------------------------------------------------------------- */
+#define GFT_MSBFS_SYMMETRIC 1u
+GFT_API size_t gft_msbfs_plane_bytes(uint32_t nnodes, uint32_t k);
+GFT_API gft_status gft_msbfs(gft_engine *e, const gft_graph *g, const uint32_t *h_sources, uint32_t k,
+                             uint32_t *d_planes, uint32_t max_levels, uint32_t flags, void *stream, gft_stats *stats);
+GFT_API gft_status gft_msbfs_levels(const uint32_t *d_planes, uint32_t nnodes, uint32_t k, uint32_t levels, uint32_t i,
+                                    int32_t *d_out, void *stream);
 
 /* Reach statistics of a result already on the device: V_r (vertices with a
  * finite value) and E_r (sum of their out-degrees, the edges a top-down

@@ -1,0 +1,77 @@
+"""Serving with continuous batching: every result of a request served in a
+mix of concurrent requests equals the same query run alone (bit for bit),
+requests really are batched and overlapped, and admission errors are
+statuses."""
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def test_mix_equals_alone(gft, engine):
+    import torch
+
+    from galoisgpu_b200.serve import Server
+
+    hosts = [gft.CSRGraph.road(60, seed=21), gft.CSRGraph.road(200, seed=22), gft.CSRGraph.rmat(11, 8, seed=23, max_weight=255),
+             gft.CSRGraph.rmat(14, 8, seed=24, max_weight=255), gft.CSRGraph.grid(30, 30, 0, 7)]
+    devs = [h.copy_to_gpu() for h in hosts]
+    # Queries on the 2^14- and 40,000-vertex graphs run on CTA groups (except
+    # BFS on the sparse road graph), the rest on one CTA each.
+    srv = Server(engine, max_batch=16, group_min_nodes=1 << 14, group_blocks=8, lane_arena_bytes=64 << 20)
+    reqs = []
+    for i in range(120):
+        gi = i % len(devs)
+        src = hosts[gi].pick_sources(300 + i, 1)[0]
+        app = "sssp" if i % 3 else "bfs"
+        out = torch.full((devs[gi].nnodes,), -5, dtype=torch.int32, device="cuda")
+        t = srv.enqueue(devs[gi], app, src, out, delta=[100, 40000][i % 2])
+        reqs.append((t, gi, app, src, out, [100, 40000][i % 2]))
+    got = {}
+    while len(got) < len(reqs):
+        for c in srv.poll(256, 100000):
+            got[c["ticket"]] = c
+    st = srv.stats()
+    srv.close()
+    assert all(c["status"] == 0 for c in got.values())
+    assert max(c["batch_size"] for c in got.values()) > 1, "requests were never batched"
+    assert len({c["lane"] for c in got.values()}) > 1, "micro-batches never overlapped on several lanes"
+    assert st["batches"] < st["queries"]
+    for t, gi, app, src, out, delta in reqs:
+        alone = (engine.sssp(devs[gi], src, delta=delta) if app == "sssp" else engine.bfs(devs[gi], src))["out"]
+        np.testing.assert_array_equal(out.cpu().numpy(), alone.cpu().numpy())
+
+
+def test_admission_errors(gft, engine):
+    import torch
+
+    from galoisgpu_b200.serve import Server
+
+    h = gft.CSRGraph.road(300, seed=3)
+    d = h.copy_to_gpu()
+    srv = Server(engine, lanes=1, lane_arena_bytes=1 << 16)
+    out = torch.empty(d.nnodes, dtype=torch.int32, device="cuda")
+    with pytest.raises(gft.GftError) as ei:
+        srv.enqueue(d, "sssp", 0, out)
+    assert ei.value.status_name == "GFT_ERR_OOM"
+    with pytest.raises(gft.GftError) as ei:
+        srv.enqueue(d, "bfs", d.nnodes, out)
+    assert ei.value.status_name == "GFT_ERR_INVALID_ARG"
+    srv.close()
+
+
+def test_poisson_load_smoke(gft, engine):
+    import torch
+
+    from galoisgpu_b200.serve import Server, poisson_run
+
+    hosts = [gft.CSRGraph.road(100, seed=31), gft.CSRGraph.rmat(12, 8, seed=32, max_weight=255)]
+    devs = [h.copy_to_gpu() for h in hosts]
+    srcs = [h.pick_sources(5, 64) for h in hosts]
+    pools = [[torch.empty(d.nnodes, dtype=torch.int32, device="cuda") for _ in range(32)] for d in devs]
+    srv = Server(engine, lanes=2, max_batch=64)
+    r = poisson_run(srv, devs, srcs, pools, rate=2000, n_requests=400)
+    srv.close()
+    assert r["failures"] == 0 and r["requests"] == 400
+    assert r["p99_ms"] is not None and r["p99_ms"] >= r["p50_ms"] > 0
