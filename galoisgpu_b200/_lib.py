@@ -138,6 +138,7 @@ class ServeConfig(C.Structure):
         ("group_min_nodes", C.c_uint32),
         ("sparse_degree", C.c_uint32),
         ("queue_capacity", C.c_uint32),
+        ("max_lanes_per_request", C.c_uint32),
     ]
 
 
@@ -149,6 +150,7 @@ class Completion(C.Structure):
         ("queue_ms", C.c_double),
         ("lane", C.c_uint32),
         ("batch_size", C.c_uint32),
+        ("width", C.c_uint32),
         ("levels", C.c_uint32),
         ("edges_scanned", C.c_uint64),
     ]

@@ -124,7 +124,7 @@ def build(force: bool = False, verbose: bool = False, ptxas_verbose: bool = Fals
         for app in ("bfs", "sssp"):
             cli_obj = BUILD / f"cli_{app}.o"
             if force or _newer(cli_obj, [cli_src, INCLUDE / "gft.h"]):
-                _run(["g++", *CXX_FLAGS, f"-DGFT_APP_SSSP={int(app == 'sssp')}", "-c", str(cli_src), "-o",
+                _run(["g++", *CXX_FLAGS, f"-DGFT_CLI_SSSP={int(app == 'sssp')}", "-c", str(cli_src), "-o",
                       str(cli_obj)], verbose)
             exe = BIN / app
             if force or _newer(exe, [cli_obj, LIB]):

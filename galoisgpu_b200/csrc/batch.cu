@@ -4,11 +4,18 @@
 // The reference runs one query per process and one persistent grid per
 // query (skelapp/skel.cu:139-151, apps/sssp/kernel.cu:426-454).  Most queries
 // of a mixed batch are small or high-diameter and cannot keep 148 SMs busy,
-// so here every query runs on ONE CTA (CtaMode: control block in shared
-// memory, __syncthreads as the barrier, no grid-wide atomics) and the CTAs
-// of one launch take queries from a device job table, largest first (longest
-// processing time first keeps the tail short).  The launch is an ordinary
-// (non-cooperative) kernel: CTAs never wait on each other.
+// so one launch runs them side by side in two phases:
+//   phase 1: queries on graphs of at least `group_min_nodes` vertices run on
+//            groups of `group` consecutive CTAs (GridMode over the group,
+//            control block in global memory, one per group); the launch is
+//            cooperative whenever there are such queries, so a group is
+//            co-resident and its bounded barrier cannot wait on a CTA that
+//            never starts;
+//   phase 2: the rest run on ONE CTA each (CtaMode: control block in shared
+//            memory, __syncthreads as the barrier, no grid-wide atomics).
+// Both phases take queries from a device job table, largest first (longest
+// processing time first keeps the tail short), and a CTA whose group finds
+// no large query left moves on to phase 2 at once.
 //
 // The job table is copied from pinned host memory by the first node of the
 // captured graph, so changing a query's source between replays needs no

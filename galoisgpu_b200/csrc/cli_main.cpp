@@ -21,12 +21,12 @@
 
 #include "gft.h"
 
-#ifndef GFT_APP_SSSP
-#define GFT_APP_SSSP 0
+#ifndef GFT_CLI_SSSP
+#define GFT_CLI_SSSP 0
 #endif
 
-static const char *kAppOpts = GFT_APP_SSSP ? "ls:d:" : "ls:";
-static const char *kAppUsage = GFT_APP_SSSP ? "[-l] [-d delta] [-s startNode]" : "[-l] [-s startNode]";
+static const char *kAppOpts = GFT_CLI_SSSP ? "ls:d:" : "ls:";
+static const char *kAppUsage = GFT_CLI_SSSP ? "[-l] [-d delta] [-s startNode]" : "[-l] [-s startNode]";
 static const char *kAppArgsUsage = "-l: enable thread block load balancer (by default false)";
 
 static void usage(const char *argv0)
@@ -97,7 +97,7 @@ int main(int argc, char **argv)
     const char *input = argv[optind];
 
     fprintf(stderr, "OPTIONS: gft engine (libgft %d, sm_100a persistent %s)\n", gft_version(),
-            GFT_APP_SSSP ? "near-far SSSP" : "BFS");
+            GFT_CLI_SSSP ? "near-far SSSP" : "BFS");
     gft_csr h;
     uint64_t t0 = now_ns();
     gft_status s = gft_gr_read(input, &h);
@@ -119,15 +119,15 @@ int main(int argc, char **argv)
     gft_stats st;
     memset(&st, 0, sizeof st);
     uint64_t k0 = now_ns();
-    if (GFT_APP_SSSP) {
+    if (GFT_CLI_SSSP) {
         printf("delta: %d\n", delta);
         s = gft_sssp_host(e, g, (uint32_t)start_node, delta, val.data(), nullptr, nullptr, nullptr, &st);
     } else {
         s = gft_bfs_host(e, g, (uint32_t)start_node, val.data(), nullptr, nullptr, nullptr, &st);
     }
     uint64_t k1 = now_ns();
-    if (s != GFT_OK) return die(GFT_APP_SSSP ? "sssp" : "bfs", s);
-    if (GFT_APP_SSSP) printf("iterations: %u\n", st.levels);
+    if (s != GFT_OK) return die(GFT_CLI_SSSP ? "sssp" : "bfs", s);
+    if (GFT_CLI_SSSP) printf("iterations: %u\n", st.levels);
     printf("gg_main %llu %llu\n", (unsigned long long)k0, (unsigned long long)k1);
     fprintf(stderr, "Total time: %llu ms\n", (unsigned long long)((k1 - k0) / 1000000));
     fprintf(stderr, "Total time: %llu ns\n", (unsigned long long)(k1 - k0));

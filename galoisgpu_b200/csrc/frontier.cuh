@@ -304,6 +304,9 @@ __device__ __forceinline__ void expand_hubs(Vis &vis, const TravParams &p, unsig
 
 __device__ __forceinline__ unsigned pick_grain(unsigned n, unsigned nwarps)
 {
+    // A frontier smaller than one 32-vertex chunk per warp is spread over
+    // all warps, so a narrow frontier is not left to a few of them.
+    if (n < nwarps * 32u) return max(1u, (n + nwarps - 1) / nwarps);
     unsigned per = n / (nwarps * 32u * 4u);
     return 32u * max(1u, min(8u, per));
 }

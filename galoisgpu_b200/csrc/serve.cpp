@@ -2,20 +2,25 @@
 // (gft_serve_*).  No counterpart in the reference, which runs one query per
 // process (skelapp/skel.cu:139-151).
 //
-// The device's resident CTAs are split into lanes of `group_blocks` CTAs,
-// each with its own stream, job table and scratch arena; the lanes' launches
-// fit side by side, so their work overlaps on the device.  A dispatcher
-// thread hands work to every free lane, in arrival order: a heavy request
-// (a graph of at least `group_min_nodes` vertices, except BFS on a graph
-// whose average degree is below `sparse_degree` when that is non-zero) gets
-// a launch of its own that runs it on the lane's whole CTA group; light
-// requests are packed into one micro-batch that runs them one CTA each.
+// The device's resident CTAs are split into lanes of `lane_blocks` CTAs,
+// each with its own stream, job table and scratch arena; launches on
+// different lanes fit side by side, so their work overlaps on the device.
+// A dispatcher thread hands work to free lanes in arrival order:
+//   * a heavy request (a graph of at least `group_min_nodes` vertices,
+//     except BFS on a graph whose average degree is below `sparse_degree`
+//     when that is non-zero) runs alone as ONE CTA group spanning w free
+//     lanes, w = free lanes / heavy requests waiting (at least 1): an idle
+//     server gives a request the whole device, so its latency is that of
+//     the query run alone, and under load requests share the device lane by
+//     lane, which overlaps the latency-bound levels of many traversals;
+//   * light requests are packed into one micro-batch on one lane, one CTA
+//     each.
 // A request that arrives while others run starts as soon as a lane and
-// arena space are free, and a long request never holds up a launch of
-// short ones.  Admission is against memory: a request is taken only if its
-// scratch fits in the lane's arena, and refused at enqueue if it could never
-// fit.  Latency is measured from enqueue to the moment the dispatcher sees
-// the request's launch complete.
+// arena space are free, and a long request never holds up a launch of short
+// ones.  Admission is against memory: a request is taken only if its scratch
+// fits in a lane's arena, and refused at enqueue if it could never fit.
+// Latency is measured from enqueue to the moment the dispatcher sees the
+// request's launch complete.
 #include <string.h>
 
 #include <algorithm>
@@ -40,7 +45,7 @@ double now_ms()
 struct Req {
     gft_query q;
     double t_arrive = 0, t_start = 0;
-    uint32_t lane = 0, batch = 0;
+    uint32_t lane = 0, batch = 0, width = 1;
 };
 
 struct Lane {
@@ -53,6 +58,7 @@ struct Lane {
     gft::TraversalCtl *d_gctl = nullptr;  // one per CTA group
     std::vector<uint64_t> tickets;        // in job-table order
     bool busy = false;
+    int owner = -1;  // lent to the launch on lane `owner`
 };
 
 }  // namespace
@@ -61,7 +67,6 @@ struct gft_server {
     gft_engine *engine = nullptr;
     gft_serve_config cfg{};
     int occ = 0;
-    uint32_t max_groups = 0;
     std::vector<Lane> lanes;
     std::mutex mu;
     std::condition_variable cv_work, cv_done;
@@ -104,6 +109,7 @@ static void complete(gft_server *s, uint64_t t, gft_status st, uint32_t levels, 
     c.queue_ms = it->second.t_start - it->second.t_arrive;
     c.lane = it->second.lane;
     c.batch_size = it->second.batch;
+    c.width = it->second.width;
     c.levels = levels;
     c.edges_scanned = edges;
     s->done.push_back(c);
@@ -112,11 +118,15 @@ static void complete(gft_server *s, uint64_t t, gft_status st, uint32_t levels, 
 }
 
 // Launches one micro-batch on lane `li`: group queries first in the job table.
-static void launch_lane(gft_server *s, uint32_t li, std::vector<uint64_t> &big, std::vector<uint64_t> &small)
+// A heavy request (big, one entry) runs as one group over `width` lanes:
+// lane `li` and the lanes in `lent`, which stay busy until `li` completes.
+static void launch_lane(gft_server *s, uint32_t li, std::vector<uint64_t> &big, std::vector<uint64_t> &small,
+                        const std::vector<uint32_t> &lent)
 {
     Lane &l = s->lanes[li];
     const uint32_t n = (uint32_t)(big.size() + small.size());
-    const uint32_t G = s->cfg.group_blocks;
+    const uint32_t width = 1 + (uint32_t)lent.size();
+    const uint32_t G = big.empty() ? s->cfg.group_blocks : width * s->cfg.lane_blocks;
     const double t = now_ms();
     size_t off = 0;
     l.tickets.clear();
@@ -130,12 +140,13 @@ static void launch_lane(gft_server *s, uint32_t li, std::vector<uint64_t> &big, 
             r.t_start = t;
             r.lane = li + 1;
             r.batch = n;
+            r.width = width;
             l.tickets.push_back(tk);
         }
     const uint32_t nbig = (uint32_t)big.size();
-    const int blocks = std::min((int)s->cfg.lane_blocks, (int)(nbig * G + small.size()));
+    const int blocks = nbig ? (int)G : std::min((int)s->cfg.lane_blocks, (int)small.size());
     cudaError_t e = cudaMemcpyAsync(l.d_jobs, l.h_jobs, sizeof(BatchJob) * n, cudaMemcpyHostToDevice, l.stream);
-    if (e == cudaSuccess && nbig) e = cudaMemsetAsync(l.d_gctl, 0, sizeof(TraversalCtl) * s->max_groups, l.stream);
+    if (e == cudaSuccess && nbig) e = cudaMemsetAsync(l.d_gctl, 0, sizeof(TraversalCtl), l.stream);
     gft_status st = e == cudaSuccess ? launch_batch_jobs(l.d_jobs, n, nbig, G, l.d_cursor, l.d_arena,
                                                          s->cfg.hub_degree, l.d_gctl, (int)s->cfg.block_threads,
                                                          blocks, l.stream)
@@ -149,6 +160,10 @@ static void launch_lane(gft_server *s, uint32_t li, std::vector<uint64_t> &big, 
         return;
     }
     l.busy = true;
+    for (uint32_t b : lent) {
+        s->lanes[b].busy = true;
+        s->lanes[b].owner = (int)li;
+    }
     s->launched_batches++;
     s->launched_queries += n;
 }
@@ -164,10 +179,10 @@ static void dispatcher_loop(gft_server *s)
             for (auto &l : s->lanes) any_busy |= l.busy;
             if (!any_busy) break;
         }
-        // Completions.
+        // Completions; a finished launch also returns the lanes lent to it.
         for (uint32_t li = 0; li < s->lanes.size(); li++) {
             Lane &l = s->lanes[li];
-            if (!l.busy) continue;
+            if (!l.busy || l.owner >= 0) continue;
             cudaError_t q = cudaEventQuery(l.done);
             if (q == cudaErrorNotReady) continue;
             const double t = now_ms();
@@ -178,19 +193,37 @@ static void dispatcher_loop(gft_server *s)
             }
             l.tickets.clear();
             l.busy = false;
+            for (auto &b : s->lanes)
+                if (b.owner == (int)li) {
+                    b.owner = -1;
+                    b.busy = false;
+                }
             idle = false;
         }
         if (!s->done.empty()) s->cv_done.notify_all();
-        // Dispatch, in arrival order: a heavy request gets a free lane to
-        // itself; a run of light requests shares one launch.
-        for (uint32_t li = 0; li < s->lanes.size() && !s->pending.empty(); li++) {
-            if (s->lanes[li].busy) continue;
-            size_t used = 0;
+        // Dispatch, in arrival order: a heavy request runs alone on a fair
+        // share of the free lanes; a run of light requests shares one lane.
+        std::vector<uint32_t> free_lanes;
+        for (uint32_t li = 0; li < s->lanes.size(); li++)
+            if (!s->lanes[li].busy) free_lanes.push_back(li);
+        size_t fi = 0;
+        while (fi < free_lanes.size() && !s->pending.empty()) {
             std::vector<uint64_t> big, small;
+            std::vector<uint32_t> lent;
+            const uint32_t li = free_lanes[fi++];
             if (runs_on_group(s, s->reqs[s->pending.front()].q)) {
+                // Heavy requests waiting, counted over a bounded window.
+                size_t heavy = 0, seen = 0;
+                for (auto it = s->pending.begin(); it != s->pending.end() && seen < 4 * s->lanes.size(); ++it, ++seen)
+                    heavy += runs_on_group(s, s->reqs[*it].q);
+                const size_t avail = free_lanes.size() - (fi - 1);
+                size_t w = std::max<size_t>(1, avail / std::max<size_t>(1, heavy));
+                w = std::min<size_t>(w, s->cfg.max_lanes_per_request);
+                while (lent.size() + 1 < w) lent.push_back(free_lanes[fi++]);
                 big.push_back(s->pending.front());
                 s->pending.pop_front();
             } else {
+                size_t used = 0;
                 while (!s->pending.empty() && small.size() < s->cfg.max_batch) {
                     const uint64_t tk = s->pending.front();
                     const Req &r = s->reqs[tk];
@@ -202,8 +235,8 @@ static void dispatcher_loop(gft_server *s)
                     s->pending.pop_front();
                 }
             }
-            if (big.empty() && small.empty()) continue;
-            launch_lane(s, li, big, small);
+            if (big.empty() && small.empty()) break;
+            launch_lane(s, li, big, small, lent);
             idle = false;
         }
         if (idle) s->cv_work.wait_for(lk, std::chrono::microseconds(20));
@@ -226,6 +259,7 @@ gft_status gft_serve_config_default(gft_serve_config *cfg)
     cfg->group_min_nodes = 1u << 18;
     cfg->sparse_degree = 0;
     cfg->queue_capacity = 1u << 20;
+    cfg->max_lanes_per_request = 0;  // all lanes
     return GFT_OK;
 }
 
@@ -254,7 +288,8 @@ gft_status gft_serve_open(gft_engine *e, const gft_serve_config *cfg_in, gft_ser
     if (s->cfg.lanes == 0) s->cfg.lanes = std::max(1u, (uint32_t)resident / s->cfg.lane_blocks);
     if (s->cfg.lanes * s->cfg.lane_blocks > (uint32_t)resident)
         s->cfg.lanes = std::max(1u, (uint32_t)resident / s->cfg.lane_blocks);
-    s->max_groups = s->cfg.group_blocks > 1 ? s->cfg.lane_blocks / s->cfg.group_blocks : 0;
+    if (s->cfg.max_lanes_per_request == 0 || s->cfg.max_lanes_per_request > s->cfg.lanes)
+        s->cfg.max_lanes_per_request = s->cfg.lanes;
     cudaError_t err = cudaSetDevice(e->device);
     s->lanes.resize(s->cfg.lanes);
     for (auto &l : s->lanes) {
@@ -264,7 +299,7 @@ gft_status gft_serve_open(gft_engine *e, const gft_serve_config *cfg_in, gft_ser
         if (err == cudaSuccess) err = cudaMalloc(&l.d_jobs, sizeof(BatchJob) * s->cfg.max_batch);
         if (err == cudaSuccess) err = cudaMalloc(&l.d_cursor, 2 * sizeof(unsigned));
         if (err == cudaSuccess) err = cudaMalloc(&l.d_arena, s->cfg.lane_arena_bytes);
-        if (err == cudaSuccess) err = cudaMalloc(&l.d_gctl, sizeof(TraversalCtl) * std::max(1u, s->max_groups));
+        if (err == cudaSuccess) err = cudaMalloc(&l.d_gctl, sizeof(TraversalCtl));
     }
     if (err != cudaSuccess) {
         gft_status st = fail(err == cudaErrorMemoryAllocation ? GFT_ERR_OOM : GFT_ERR_CUDA, "gft_serve_open: %s",

@@ -2,11 +2,12 @@
 (the gft_serve_* C ABI), plus a Poisson load generator that reports
 throughput and p50/p99 latency.
 
-Requests are packed, as they arrive, into micro-batches that run on several
-lanes (streams), each on its share of the device's CTAs, so requests that
-arrive while others are on the GPU start as soon as a lane and scratch
-memory are free.  Large queries run on CTA groups, small ones (and BFS on
-sparse graphs) on one CTA each.  See include/gft.h.
+The server splits the device's CTAs into lanes (streams).  A large query
+runs alone as one CTA group over a fair share of the free lanes (the whole
+device when the server is idle, one lane under load); small queries are
+packed into micro-batches on one lane, one CTA each.  Requests that arrive
+while others are on the GPU start as soon as a lane and scratch memory are
+free.  See include/gft.h.
 """
 
 from __future__ import annotations
@@ -90,7 +91,7 @@ def poisson_run(server: Server, graphs: list[DeviceGraph], sources: list[list[in
     free = [list(range(len(p))) for p in pools]
     lock = threading.Lock()
     busy = {}  # ticket -> (graph index, buffer index)
-    lat, qms, lanes, bsz = [], [], {}, []
+    lat, qms, lanes, bsz, width = [], [], {}, [], []
     failures = 0
     done = [0]
     stop = [False]
@@ -108,6 +109,7 @@ def poisson_run(server: Server, graphs: list[DeviceGraph], sources: list[list[in
                 qms.append(c["queue_ms"])
                 lanes[c["lane"]] = lanes.get(c["lane"], 0) + 1
                 bsz.append(c["batch_size"])
+                width.append(c["width"])
                 done[0] += 1
             if stop[0] and done[0] >= n_requests:
                 break
@@ -159,6 +161,7 @@ def poisson_run(server: Server, graphs: list[DeviceGraph], sources: list[list[in
         "p99_ms": _pct(lat, 0.99),
         "queue_p50_ms": _pct(qms, 0.5),
         "mean_batch": sum(bsz) / max(1, len(bsz)),
+        "mean_width": sum(width) / max(1, len(width)),
         "lanes": lanes,
         "throttled_arrivals": throttled,
         "failures": failures,

@@ -288,13 +288,15 @@ GFT_API void gft_batch_destroy(gft_batch *b);
 /* ---------------------------------------------------------------------------
  * Serving (no counterpart in the reference, which runs one query per
  * process).  A request loop over resident graphs with continuous batching.
- * The device's resident CTAs are split into `lanes` of `lane_blocks` CTAs
- * (default: one lane per group of `group_blocks` CTAs), each with its own
- * stream and scratch arena, so their launches overlap on the device.  In
- * arrival order, a heavy request (a graph of at least `group_min_nodes`
- * vertices; with sparse_degree > 0, BFS on a graph of lower average degree
- * counts as light) gets a free lane to itself and runs on its CTA group;
- * a run of light requests shares one launch, one CTA each.  A request that
+ * The device's resident CTAs are split into `lanes` of `lane_blocks` CTAs,
+ * each with its own stream and scratch arena, so their launches overlap on
+ * the device.  In arrival order, a heavy request (a graph of at least
+ * `group_min_nodes` vertices; with sparse_degree > 0, BFS on a graph of
+ * lower average degree counts as light) runs alone as one CTA group over
+ * w free lanes, w = free lanes / heavy requests waiting, at least 1 and at
+ * most `max_lanes_per_request`: on an idle server a request gets the whole
+ * device, under load requests share it lane by lane.  A run of light
+ * requests shares one launch on one lane, one CTA each.  A request that
  * arrives while others run starts as soon as a lane and arena space are
  * free, and a long request never holds up a launch of short ones.  A
  * request is taken only when its scratch fits in the lane's arena
@@ -309,10 +311,11 @@ typedef struct gft_serve_config {
     uint32_t block_threads;     /* CTA size (default 512)                        */
     uint32_t hub_degree;        /* default 256                                   */
     uint32_t lane_blocks;       /* CTAs per lane (0 = group_blocks)              */
-    uint32_t group_blocks;      /* CTAs per heavy request (default 16)           */
+    uint32_t group_blocks;      /* default lane size in CTAs (default 16)        */
     uint32_t group_min_nodes;   /* default 2^18                                  */
     uint32_t sparse_degree;     /* default 0 (no exception)                      */
     uint32_t queue_capacity;    /* requests admitted but not completed           */
+    uint32_t max_lanes_per_request; /* widest heavy launch (0 = all lanes)       */
 } gft_serve_config;
 
 typedef struct gft_completion {
@@ -322,6 +325,7 @@ typedef struct gft_completion {
     double queue_ms;        /* enqueue -> launch                              */
     uint32_t lane;          /* lane (1-based) that ran the request             */
     uint32_t batch_size;    /* requests in the same launch                    */
+    uint32_t width;         /* lanes the launch spanned                       */
     uint32_t levels;
     uint64_t edges_scanned;
 } gft_completion;

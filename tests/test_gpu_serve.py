@@ -43,6 +43,24 @@ def test_mix_equals_alone(gft, engine):
         np.testing.assert_array_equal(out.cpu().numpy(), alone.cpu().numpy())
 
 
+def test_idle_server_gives_a_heavy_request_the_device(gft, engine):
+    import torch
+
+    from galoisgpu_b200.serve import Server
+
+    h = gft.CSRGraph.road(200, seed=5)
+    d = h.copy_to_gpu()
+    srv = Server(engine, group_min_nodes=1 << 12, group_blocks=8, lane_arena_bytes=64 << 20)
+    out = torch.empty(d.nnodes, dtype=torch.int32, device="cuda")
+    srv.enqueue(d, "sssp", 3, out, delta=1000)
+    got = []
+    while not got:
+        got = srv.poll(4, 100000)
+    srv.close()
+    assert got[0]["status"] == 0 and got[0]["width"] > 1
+    np.testing.assert_array_equal(out.cpu().numpy(), engine.sssp(d, 3, delta=1000)["out"].cpu().numpy())
+
+
 def test_admission_errors(gft, engine):
     import torch
 
