@@ -192,6 +192,11 @@ def profile_traffic(workload: str, kernel: str) -> tuple[float | None, str | Non
 
 
 def algorithmic_bytes(app: str, v_r: int, e_r: int) -> int:
+    """Bytes a traversal must move: per edge, its destination (+ weight for
+    SSSP) and one probe of the destination's state; per reached vertex, its
+    row_start pair, result write and queue push and pop.  For BFS, e_r is
+    the edges actually examined: all reached edges top-down, fewer when
+    bottom-up levels stop at the first parent found."""
     return (12 if app == "sssp" else 8) * e_r + 20 * v_r
 
 
@@ -253,9 +258,11 @@ def bench_workload(gft, name: str, steps: int, warmup: int, d, dev: int, headlin
     # Per-source reach statistics (E_r, V_r) from the first run of each source.
     reach = {}
     qstats = []
+    scanned = {}
     for s in sources:
         run_queries(gft, eng, dg, spec, [s], out, stream, tune, delta, qstats)
         reach[s] = gft.reach_stats(dg, out, stream)
+        scanned[s] = qstats[-1]["edges_scanned"]
     step_src = [sources[i % len(sources)] for i in range(max(steps, len(sources)))]
     timed_src = step_src[:steps] if len(sources) <= steps else sources
     k = len(timed_src)
@@ -295,7 +302,8 @@ def bench_workload(gft, name: str, steps: int, warmup: int, d, dev: int, headlin
     e2e_value = d.world * sum(reach[s][1] for s in e2e_src) / (e2e_s * 1e9)
 
     peak, peak_kind = measured_peaks()
-    alg_bytes = algorithmic_bytes(app, v_sum, e_sum) / k
+    e_alg = e_sum if app == "sssp" else sum(min(reach[s][1], scanned[s]) for s in timed_src)
+    alg_bytes = algorithmic_bytes(app, v_sum, e_alg) / k
     achieved = alg_bytes / (kernel_ms * 1e-3) / 1e9
     kname = f"{app}_persistent"
     traffic, traffic_src = profile_traffic(name, kname)

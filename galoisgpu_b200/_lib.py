@@ -75,6 +75,7 @@ class Tuning(C.Structure):
         ("max_blocks", C.c_uint32),
         ("group_blocks", C.c_uint32),
         ("group_min_nodes", C.c_uint32),
+        ("direction", C.c_uint32),
     ]
 
 
@@ -177,6 +178,8 @@ _SIGS: dict[str, tuple] = {
     "gft_graph_generate": (C.c_int, [C.c_int, C.POINTER(GenParams), _P, C.POINTER(_P)]),
     "gft_graph_info": (C.c_int, [_P, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.POINTER(C.c_int)]),
     "gft_graph_arrays": (C.c_int, [_P, C.POINTER(_P), C.POINTER(_P), C.POINTER(_P)]),
+    "gft_graph_set_symmetric": (C.c_int, [_P, C.c_int]),
+    "gft_graph_is_symmetric": (C.c_int, [_P, C.POINTER(C.c_int)]),
     "gft_graph_download": (C.c_int, [_P, C.POINTER(Csr)]),
     "gft_graph_pick_sources": (C.c_int, [_P, C.c_uint64, C.c_uint32, C.POINTER(C.c_uint32)]),
     "gft_graph_free": (None, [_P]),

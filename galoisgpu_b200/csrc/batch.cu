@@ -54,6 +54,8 @@ __device__ __forceinline__ TravParams job_params(const BatchJob &jb, char *scrat
     p.ctl = ctl;
     p.skip_block = -1;
     p.vec_ok = jb.vec_ok;
+    p.uniform = jb.uniform;
+    p.nedges = jb.nedges;
     if (jb.app == 1) {
         p.far[0] = reinterpret_cast<uint32_t *>(base + 2 * qbytes);
         p.far[1] = reinterpret_cast<uint32_t *>(base + 3 * qbytes);
@@ -92,8 +94,8 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK)
                  uint32_t hub_degree, TraversalCtl *gctl, unsigned long long timeout_ns)
 {
     __shared__ TraversalCtl s_ctl;
-    __shared__ uint32_t s_near[BLOCK / 32][64];
-    __shared__ uint32_t s_far[BLOCK / 32][64];
+    __shared__ uint32_t s_near[BLOCK / 32][kQueueBuf];
+    __shared__ uint32_t s_far[BLOCK / 32][kQueueBuf];
     __shared__ unsigned s_job;
     const unsigned w = threadIdx.x >> 5;
 
@@ -237,6 +239,7 @@ void fill_batch_job(BatchJob &j, const gft_query &x, uint32_t hub_degree)
     j.app = x.app;
     j.hub_cap = (uint32_t)std::min<uint64_t>(G.nnodes, (uint64_t)G.nedges / hub_degree + 1);
     j.vec_ok = ((uintptr_t)G.edge_dst % 16 == 0) && (!G.edge_data || (uintptr_t)G.edge_data % 16 == 0);
+    j.uniform = G.max_degree <= kUniformDegree;
 }
 
 // Bytes of scratch one CTA-mode job needs (layout of batch_kernel).

@@ -42,6 +42,35 @@ void Scratch::release()
     bytes = 0;
 }
 
+namespace dev {
+__global__ void max_degree_kernel(const uint32_t *__restrict__ row_start, uint32_t n, unsigned *out)
+{
+    unsigned m = 0;
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x)
+        m = max(m, row_start[v + 1] - row_start[v]);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(0xFFFFFFFFu, m, o));
+    if ((threadIdx.x & 31) == 0 && m) atomicMax(out, m);
+}
+}  // namespace dev
+
+gft_status graph_degree_stats(DeviceGraph &G, cudaStream_t stream)
+{
+    unsigned *d = nullptr, h = 0;
+    GFT_CUDA_TRY(cudaMallocAsync(&d, sizeof(unsigned), stream));
+    cudaError_t err = cudaMemsetAsync(d, 0, sizeof(unsigned), stream);
+    if (err == cudaSuccess && G.nnodes) {
+        dev::max_degree_kernel<<<592, 256, 0, stream>>>(G.row_start, G.nnodes, d);
+        err = cudaGetLastError();
+    }
+    if (err == cudaSuccess) err = cudaMemcpyAsync(&h, d, sizeof(unsigned), cudaMemcpyDeviceToHost, stream);
+    cudaFreeAsync(d, stream);
+    if (err == cudaSuccess) err = cudaStreamSynchronize(stream);
+    GFT_CUDA_TRY(err);
+    G.max_degree = h;
+    return GFT_OK;
+}
+
 gft_status resolve_shape(gft_engine *e, const void *kernel, int block_threads, int blocks_per_sm, size_t dyn_smem,
                          LaunchShape *out)
 {
@@ -161,6 +190,7 @@ gft_status gft_graph_upload(int device, const gft_csr *h, void *stream_, gft_gra
         return fail(err == cudaErrorMemoryAllocation ? GFT_ERR_OOM : GFT_ERR_CUDA, "gft_graph_upload: %s",
                     cudaGetErrorString(err));
     }
+    for (uint32_t v = 0; v < h->nnodes; v++) G.max_degree = std::max(G.max_degree, h->row_start[v + 1] - h->row_start[v]);
     *out = g;
     return GFT_OK;
 }
@@ -179,7 +209,27 @@ gft_status gft_graph_wrap(int device, uint32_t nnodes, uint32_t nedges, const ui
     g->g.edge_dst = const_cast<uint32_t *>(d_edge_dst);
     g->g.edge_data = const_cast<int32_t *>(d_edge_data);
     g->g.wrapped = true;
+    gft_status st = cudaSetDevice(device) == cudaSuccess ? graph_degree_stats(g->g, nullptr)
+                                                           : fail(GFT_ERR_CUDA, "gft_graph_wrap: cudaSetDevice failed");
+    if (st != GFT_OK) {
+        delete g;
+        return st;
+    }
     *out = g;
+    return GFT_OK;
+}
+
+gft_status gft_graph_set_symmetric(gft_graph *g, int symmetric)
+{
+    if (!g) return fail(GFT_ERR_INVALID_ARG, "gft_graph_set_symmetric: graph is NULL");
+    g->g.symmetric = symmetric != 0;
+    return GFT_OK;
+}
+
+gft_status gft_graph_is_symmetric(const gft_graph *g, int *symmetric)
+{
+    if (!g || !symmetric) return fail(GFT_ERR_INVALID_ARG, "gft_graph_is_symmetric: null argument");
+    *symmetric = g->g.symmetric ? 1 : 0;
     return GFT_OK;
 }
 

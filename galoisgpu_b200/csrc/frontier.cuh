@@ -48,6 +48,9 @@ struct TravParams {
     unsigned long long timeout_ns;
     int skip_block;
     int vec_ok;
+    uint32_t nedges;
+    int dir_opt;  // BFS: direction-optimising (graph marked symmetric)
+    int uniform;  // every out-degree <= kUniformDegree: static chunks
 };
 
 // ---------------------------------------------------------------------------
@@ -57,8 +60,33 @@ struct BfsOwn {
     uint32_t u;
 };
 
+#ifndef GFT_BFS_BATCH
+#define GFT_BFS_BATCH 2
+#endif
+#ifndef GFT_SSSP_BATCH
+#define GFT_SSSP_BATCH 2
+#endif
+
+#ifdef GFT_TRACE
+// Diagnostic builds only: per-iteration (time, work) records of the last
+// single-query traversal, read back by gft_debug_trace.
+__device__ unsigned long long g_trace[2 * 8192];
+__device__ __forceinline__ void trace_iter(unsigned i, unsigned long long info)
+{
+    if (i < 8192) {
+        g_trace[2 * i] = globaltimer_ns();
+        g_trace[2 * i + 1] = info;
+    }
+}
+#else
+__device__ __forceinline__ void trace_iter(unsigned, unsigned long long) {}
+#endif
+
 struct BfsVisitor {
+    static constexpr int kBatch = GFT_BFS_BATCH;  // edges per lane in one flattened step
     const uint32_t *__restrict__ edge_dst;
+    const uint32_t *__restrict__ row_start;  // non-NULL: sum the out-degrees of claimed vertices
+    unsigned long long mf;                    // that sum, per lane
     uint32_t *visited;
     int32_t *level;
     uint32_t *parent;
@@ -75,35 +103,59 @@ struct BfsVisitor {
         return BfsOwn{__shfl_sync(kFull, o.u, lane)};
     }
 
-    __device__ __forceinline__ void visit(bool valid, uint32_t dst, const BfsOwn &o, unsigned lane)
+    // K visits per lane, staged so that the lane's K bitmap probes, then its
+    // K claims, are each in flight together: one memory latency per stage
+    // instead of one per edge.  Two of a lane's K edges may name the same
+    // vertex; the second claim then sees the first one's bit.
+    template <int K>
+    __device__ __forceinline__ void visitK(const bool (&valid)[K], const uint32_t (&dst)[K], const BfsOwn (&o)[K],
+                                           unsigned lane)
     {
-        bool mine = false;
-        if (valid) {
-            edges++;
-            uint32_t w = dst >> 5, b = 1u << (dst & 31);
-            if (!(__ldcg(visited + w) & b)) {
-                mine = !(atomicOr(visited + w, b) & b);
-                if (mine) {
-                    level[dst] = newlevel;
-                    if (parent) parent[dst] = o.u;
-                    claimed++;
-                }
-            }
+        uint32_t word[K];
+#pragma unroll
+        for (int k = 0; k < K; k++) word[k] = valid[k] ? __ldcg(visited + (dst[k] >> 5)) : 0xFFFFFFFFu;
+        bool mine[K];
+#pragma unroll
+        for (int k = 0; k < K; k++) {
+            const uint32_t b = 1u << (dst[k] & 31);
+            mine[k] = false;
+            if (valid[k]) edges++;
+            if (!(word[k] & b)) word[k] = atomicOr(visited + (dst[k] >> 5), b), mine[k] = !(word[k] & b);
         }
-        q.push(mine, dst, lane);
+#pragma unroll
+        for (int k = 0; k < K; k++) {
+            if (mine[k]) {
+                level[dst[k]] = newlevel;
+                if (parent) parent[dst[k]] = o[k].u;
+                claimed++;
+                if (row_start) mf += __ldg(row_start + dst[k] + 1) - __ldg(row_start + dst[k]);
+            }
+            q.push(mine[k], dst[k], lane);
+        }
+    }
+    template <int K>
+    __device__ __forceinline__ void edgeK(const bool (&valid)[K], const uint32_t (&e)[K], const BfsOwn (&o)[K],
+                                          unsigned lane)
+    {
+        uint32_t d[K];
+#pragma unroll
+        for (int k = 0; k < K; k++) d[k] = valid[k] ? ld_stream(edge_dst + e[k]) : 0u;
+        visitK<K>(valid, d, o, lane);
     }
     __device__ __forceinline__ void edge1(bool valid, uint32_t e, const BfsOwn &o, unsigned lane)
     {
-        uint32_t d = valid ? ld_stream(edge_dst + e) : 0u;
-        visit(valid, d, o, lane);
+        const bool v[1] = {valid};
+        const uint32_t ee[1] = {e};
+        const BfsOwn oo[1] = {o};
+        edgeK<1>(v, ee, oo, lane);
     }
     __device__ __forceinline__ void edge4(bool valid, uint32_t e, const BfsOwn &o, unsigned lane)
     {
-        uint4 d = valid ? ld_stream4(edge_dst + e) : make_uint4(0, 0, 0, 0);
-        visit(valid, d.x, o, lane);
-        visit(valid, d.y, o, lane);
-        visit(valid, d.z, o, lane);
-        visit(valid, d.w, o, lane);
+        const uint4 d = valid ? ld_stream4(edge_dst + e) : make_uint4(0, 0, 0, 0);
+        const bool v[4] = {valid, valid, valid, valid};
+        const uint32_t dd[4] = {d.x, d.y, d.z, d.w};
+        const BfsOwn oo[4] = {o, o, o, o};
+        visitK<4>(v, dd, oo, lane);
     }
 };
 
@@ -121,6 +173,7 @@ struct SsspOwn {
 // improvement above the threshold writes near_tag - 1 and is deduplicated in
 // the far pile with a per-phase stamp.
 struct SsspVisitor {
+    static constexpr int kBatch = GFT_SSSP_BATCH;  // edges per lane in one flattened step
     const uint32_t *__restrict__ edge_dst;
     const int32_t *__restrict__ edge_data;
     unsigned long long *dt;
@@ -143,39 +196,72 @@ struct SsspVisitor {
         return SsspOwn{__shfl_sync(kFull, o.u, lane), __shfl_sync(kFull, o.du, lane)};
     }
 
-    __device__ __forceinline__ void relax(bool valid, uint32_t v, uint32_t w, const SsspOwn &o, unsigned lane)
+    // K relaxations per lane, staged so that the lane's K distance probes,
+    // then its K atomicMins, then its far-pile stamps, are each in flight
+    // together: one memory latency per stage instead of one per edge.  Two of
+    // a lane's K edges may name the same vertex; its atomics then apply in
+    // program order, so the second one sees the first one's word and the
+    // vertex is queued once, as with one edge at a time.
+    template <int K>
+    __device__ __forceinline__ void relaxK(const bool (&valid)[K], const uint32_t (&v)[K], const uint32_t (&w)[K],
+                                           const SsspOwn (&o)[K], unsigned lane)
     {
-        bool to_near = false, to_far = false;
-        if (valid) {
+        unsigned long long cur[K];
+#pragma unroll
+        for (int k = 0; k < K; k++) cur[k] = valid[k] ? __ldcg(dt + v[k]) : 0ull;
+        uint32_t nd[K];
+        bool to_near[K], to_far[K];
+#pragma unroll
+        for (int k = 0; k < K; k++) {
+            to_near[k] = to_far[k] = false;
+            nd[k] = o[k].du + w[k];  // du < 2^31 and w < 2^32: a wrap is caught below
+            if (!valid[k]) continue;
             edges++;
-            uint32_t nd = o.du + w;  // du < 2^31 and w < 2^32: no wrap in 32 bits is checked below
-            if (nd >= kInf || nd < o.du) {
-                raise_error(err, err_where, GFT_ERR_OVERFLOW, o.u);
-            } else if (nd < (uint32_t)(__ldcg(dt + v) >> 32)) {
-                const bool near = nd <= threshold;
-                const unsigned long long mine = ((unsigned long long)nd << 32) | (near ? near_tag : near_tag - 1);
-                const unsigned long long old = atomicMin(dt + v, mine);
-                if (nd < (uint32_t)(old >> 32)) {
-                    if (near) {
-                        to_near = (uint32_t)old != near_tag;
-                    } else {
-                        far_min = min(far_min, nd);
-                        to_far = atomicExch(far_stamp + v, far_tag) != far_tag;
-                    }
+            if (nd[k] >= kInf || nd[k] < o[k].du) {
+                raise_error(err, err_where, GFT_ERR_OVERFLOW, o[k].u);
+            } else if (nd[k] < (uint32_t)(cur[k] >> 32)) {
+                const bool near = nd[k] <= threshold;
+                const unsigned long long mine = ((unsigned long long)nd[k] << 32) | (near ? near_tag : near_tag - 1);
+                cur[k] = atomicMin(dt + v[k], mine);
+                if (nd[k] < (uint32_t)(cur[k] >> 32)) {
+                    to_near[k] = near && (uint32_t)cur[k] != near_tag;
+                    to_far[k] = !near;
                 }
             }
         }
-        nq.push(to_near, v, lane);
-        fq.push(to_far, v, lane);
+        uint32_t stamp[K];
+#pragma unroll
+        for (int k = 0; k < K; k++) {
+            stamp[k] = far_tag;
+            if (to_far[k]) {
+                far_min = min(far_min, nd[k]);
+                stamp[k] = atomicExch(far_stamp + v[k], far_tag);
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < K; k++) {
+            nq.push(to_near[k], v[k], lane);
+            fq.push(to_far[k] && stamp[k] != far_tag, v[k], lane);
+        }
+    }
+    template <int K>
+    __device__ __forceinline__ void edgeK(const bool (&valid)[K], const uint32_t (&e)[K], const SsspOwn (&o)[K],
+                                          unsigned lane)
+    {
+        uint32_t d[K], w[K];
+#pragma unroll
+        for (int k = 0; k < K; k++) {
+            d[k] = valid[k] ? ld_stream(edge_dst + e[k]) : 0u;
+            w[k] = (valid[k] && edge_data) ? (uint32_t)__ldcs(edge_data + e[k]) : 0u;
+        }
+        relaxK<K>(valid, d, w, o, lane);
     }
     __device__ __forceinline__ void edge1(bool valid, uint32_t e, const SsspOwn &o, unsigned lane)
     {
-        uint32_t d = 0, w = 0;
-        if (valid) {
-            d = ld_stream(edge_dst + e);
-            if (edge_data) w = (uint32_t)__ldcs(edge_data + e);
-        }
-        relax(valid, d, w, o, lane);
+        const bool vv[1] = {valid};
+        const uint32_t ee[1] = {e};
+        const SsspOwn oo[1] = {o};
+        edgeK<1>(vv, ee, oo, lane);
     }
     __device__ __forceinline__ void edge4(bool valid, uint32_t e, const SsspOwn &o, unsigned lane)
     {
@@ -184,10 +270,10 @@ struct SsspVisitor {
             d = ld_stream4(edge_dst + e);
             if (edge_data) w = __ldcs(reinterpret_cast<const uint4 *>(edge_data + e));
         }
-        relax(valid, d.x, w.x, o, lane);
-        relax(valid, d.y, w.y, o, lane);
-        relax(valid, d.z, w.z, o, lane);
-        relax(valid, d.w, w.w, o, lane);
+        const bool vv[4] = {valid, valid, valid, valid};
+        const uint32_t dd[4] = {d.x, d.y, d.z, d.w}, ww[4] = {w.x, w.y, w.z, w.w};
+        const SsspOwn oo[4] = {o, o, o, o};
+        relaxK<4>(vv, dd, ww, oo, lane);
     }
 };
 
@@ -233,6 +319,37 @@ struct ChunkSched {
     }
 };
 
+// Flattened expansion of the edge ranges [start, start+deg) held one per
+// lane (thread granularity): the warp takes the ranges' edges 32 * K at a
+// time, K per lane, finds each edge's owner lane with a shuffle binary
+// search over the exclusive prefix of the degrees, and hands the lane's K
+// edges to the visitor together, so their memory operations overlap.
+template <int K, class Vis, class Own>
+__device__ __forceinline__ void flatten_edges(Vis &vis, uint32_t start, uint32_t deg, const Own &o, unsigned lane)
+{
+    const uint32_t incl = warp_incl_sum(deg, lane);
+    const uint32_t total = __shfl_sync(kFull, incl, 31);
+    const uint32_t excl = incl - deg;
+    for (uint32_t base = 0; base < total; base += 32u * K) {
+        bool valid[K];
+        uint32_t e[K];
+        Own ow[K];
+#pragma unroll
+        for (int k = 0; k < K; k++) {
+            const uint32_t g = base + 32u * k + lane;
+            int j = 0;
+#pragma unroll
+            for (int step = 16; step >= 1; step >>= 1)
+                if (__shfl_sync(kFull, excl, j + step) <= g) j += step;
+            const uint32_t ostart = __shfl_sync(kFull, start, j), oexcl = __shfl_sync(kFull, excl, j);
+            valid[k] = g < total;
+            e[k] = ostart + (g - oexcl);
+            ow[k] = vis.shfl(o, j);
+        }
+        vis.template edgeK<K>(valid, e, ow, lane);
+    }
+}
+
 // Expands the frontier `in[0, n)` in chunks of `grain` vertices.  Vertices
 // of degree >= hub_degree are recorded in the hub list for the grid-wide hub
 // phase instead.
@@ -271,7 +388,7 @@ __device__ __forceinline__ void expand_frontier(Vis &vis, const TravParams &p, c
                 warp_range(vis, s, d, vis.shfl(o, l), lane);
             }
             if (deg >= 32) deg = 0;
-            warp_flatten(start, deg, lane, [&](bool valid, int j, uint32_t e) { vis.edge1(valid, e, vis.shfl(o, j), lane); });
+            flatten_edges<Vis::kBatch>(vis, start, deg, o, lane);
         }
     }
 }
@@ -302,13 +419,71 @@ __device__ __forceinline__ void expand_hubs(Vis &vis, const TravParams &p, unsig
     }
 }
 
-__device__ __forceinline__ unsigned pick_grain(unsigned n, unsigned nwarps)
+// Chunk size (vertices) for a frontier of n vertices over nwarps warps.  A
+// frontier smaller than one 32-vertex chunk per warp is spread over all
+// warps.  On a graph of uniform degree (road networks, grids) a larger
+// frontier is cut into one chunk per warp, so no warp claims work through
+// the shared cursor, whose atomics serialise in one L2 slice; on skewed
+// graphs (R-MAT) about four chunks per warp are claimed dynamically, which
+// keeps the warps balanced.
+__device__ __forceinline__ unsigned pick_grain(unsigned n, unsigned nwarps, bool uniform)
 {
-    // A frontier smaller than one 32-vertex chunk per warp is spread over
-    // all warps, so a narrow frontier is not left to a few of them.
     if (n < nwarps * 32u) return max(1u, (n + nwarps - 1) / nwarps);
+    if (uniform) return 32u * ((n + nwarps * 32u - 1) / (nwarps * 32u));
     unsigned per = n / (nwarps * 32u * 4u);
     return 32u * max(1u, min(8u, per));
+}
+
+// One bottom-up BFS level (Beamer, Asanovic, Patterson, "Direction-Optimizing
+// Breadth-First Search", SC 2012): every unvisited vertex scans its own
+// edges, four at a time, for a neighbour in the current frontier (level ==
+// L) and stops at the first it finds.  On a symmetric graph a vertex's
+// out-edges are its in-edges, so this claims exactly the vertices a
+// top-down level would, with the same level.  Warps take 32-vertex words of
+// the visited bitmap and own them for the level, so each sets its word's
+// new bits with one plain store; claimed vertices are also queued, so a
+// top-down level can follow.
+__device__ __forceinline__ void bottom_up_level(BfsVisitor &vis, const TravParams &p, unsigned L, unsigned gwarp,
+                                                unsigned nwarps, unsigned lane)
+{
+    const uint32_t n = p.nnodes, nwords = (n + 31) >> 5;
+    const int32_t cur = (int32_t)L;
+    for (uint32_t w = gwarp; w < nwords; w += nwarps) {
+        const uint32_t word = __ldcg(p.visited + w);
+        if (word == 0xFFFFFFFFu) continue;  // warp uniform
+        const uint32_t v = (w << 5) + lane;
+        bool found = false;
+        uint32_t par = 0, deg = 0;
+        if (v < n && !((word >> lane) & 1u)) {
+            const uint32_t s = __ldg(p.row_start + v), e = __ldg(p.row_start + v + 1);
+            deg = e - s;
+            for (uint32_t i = s; i < e && !found; i += 4) {
+                uint32_t u[4];
+                int32_t lv[4];
+#pragma unroll
+                for (int k = 0; k < 4; k++) u[k] = i + k < e ? ld_stream(p.edge_dst + i + k) : 0u;
+#pragma unroll
+                for (int k = 0; k < 4; k++) lv[k] = i + k < e ? __ldcg(p.out + u[k]) : -1;
+#pragma unroll
+                for (int k = 0; k < 4; k++)
+                    if (!found && lv[k] == cur) {
+                        found = true;
+                        par = u[k];
+                        vis.edges += k + 1;
+                    }
+                if (!found) vis.edges += min(4u, e - i);
+            }
+        }
+        const uint32_t got = __ballot_sync(kFull, found);
+        if (found) {
+            p.out[v] = cur + 1;
+            if (p.parent) p.parent[v] = par;
+            vis.claimed++;
+            vis.mf += deg;
+        }
+        if (lane == 0 && got) p.visited[w] = word | got;
+        vis.q.push(found, v, lane);
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -349,6 +524,11 @@ struct CtaMode {
 // ---------------------------------------------------------------------------
 // BFS body
 // ---------------------------------------------------------------------------
+// Direction switch (Beamer et al.): go bottom-up once the frontier's edges
+// exceed 1/kAlpha of the edges still unexplored, and back top-down once the
+// frontier holds fewer than 1/kBeta of the vertices.
+constexpr unsigned kAlpha = 14, kBeta = 24;
+
 template <class Mode>
 __device__ __forceinline__ void bfs_body(const TravParams &p, Mode &m, uint32_t *warp_buf)
 {
@@ -367,11 +547,19 @@ __device__ __forceinline__ void bfs_body(const TravParams &p, Mode &m, uint32_t 
     if (tid == 0) {
         p.q[0][0] = p.src;
         *u32_of(ctl->qlen[0]) = 1;
+        // far_len[] carries, per level slot, the out-degree sum of the
+        // frontier (BFS has no far pile).
+        *u32_of(ctl->far_len[0]) = p.row_start[p.src + 1] - p.row_start[p.src];
     }
     if (!m.sync()) return;
 
     BfsVisitor vis;
     vis.edge_dst = p.edge_dst;
+    // Skewed graphs sum the claimed vertices' out-degrees for the direction
+    // switch; on uniform-degree graphs the frontier's size times the mean
+    // degree is as good and costs no loads.
+    vis.row_start = (p.dir_opt && !p.uniform) ? p.row_start : nullptr;
+    vis.mf = 0;
     vis.visited = p.visited;
     vis.level = p.out;
     vis.parent = p.parent;
@@ -385,28 +573,63 @@ __device__ __forceinline__ void bfs_body(const TravParams &p, Mode &m, uint32_t 
     vis.q.err_where = &ctl->error_where;
 
     unsigned L = 0;
+    bool bottom_up = false;
+    unsigned long long m_seen = 0;  // out-degree sum of the frontiers of finished levels
+    unsigned long long n_seen = 0;  // vertices reached so far (uniform-degree estimate)
     for (;;) {
         const unsigned slot = L % 3, nslot = (L + 1) % 3, rslot = (L + 2) % 3;
         const unsigned n_in = m.ld(u32_of(ctl->qlen[slot]));
-        if (n_in == 0) break;
+        if (n_in == 0) {
+            if (tid == 0) trace_iter(L, 0);
+            break;
+        }
+        if (p.dir_opt) {  // every thread reads the same counters: a uniform decision
+            const unsigned long long E = p.nedges;
+            unsigned long long mf, m_u;
+            if (p.uniform) {
+                n_seen += n_in;
+                mf = (unsigned long long)n_in * E / n;
+                m_u = E - min(E, n_seen * E / n);
+            } else {
+                mf = m.ld(u32_of(ctl->far_len[slot]));
+                m_u = E - min(E, m_seen + mf);
+                m_seen += mf;
+            }
+            bottom_up = bottom_up ? (unsigned long long)n_in * kBeta >= n : mf * kAlpha > m_u;
+        }
         if (tid == 0) {
+            trace_iter(L, n_in | ((unsigned long long)bottom_up << 32));
             *u32_of(ctl->qlen[rslot]) = 0;
             *u32_of(ctl->claim[rslot]) = 0;
             ctl->hub[rslot].v = 0;
             *u32_of(ctl->hub_claim[rslot]) = 0;
+            *u32_of(ctl->far_len[rslot]) = 0;
         }
         vis.newlevel = (int)L + 1;
         vis.q.queue = sel2(p.q, (L + 1));
         vis.q.len = u32_of(ctl->qlen[nslot]);
-        expand_frontier<BfsVisitor, BfsOwn>(vis, p, sel2(p.q, L), n_in, u32_of(ctl->claim[slot]), &ctl->hub[slot].v,
-                                            pick_grain(n_in, nwarps), gwarp, nwarps, lane);
+        unsigned *mf_next = u32_of(ctl->far_len[nslot]);
+        if (bottom_up) {
+            bottom_up_level(vis, p, L, gwarp, nwarps, lane);
+        } else {
+            expand_frontier<BfsVisitor, BfsOwn>(vis, p, sel2(p.q, L), n_in, u32_of(ctl->claim[slot]),
+                                                &ctl->hub[slot].v, pick_grain(n_in, nwarps, p.uniform), gwarp, nwarps, lane);
+        }
         vis.q.flush(lane);
+        if (p.dir_opt) {
+            warp_add_u32(mf_next, (unsigned)vis.mf, lane);
+            vis.mf = 0;
+        }
         if (!m.sync()) return;
-        const unsigned long long hv = m.ld64(&ctl->hub[slot].v);
+        const unsigned long long hv = bottom_up ? 0ull : m.ld64(&ctl->hub[slot].v);
         if (hv) {
             expand_hubs<BfsVisitor, BfsOwn>(vis, p, (unsigned)(hv >> 32), (unsigned)hv, u32_of(ctl->hub_claim[slot]),
                                             gwarp, nwarps, lane);
             vis.q.flush(lane);
+            if (p.dir_opt) {
+                warp_add_u32(mf_next, (unsigned)vis.mf, lane);
+                vis.mf = 0;
+            }
             if (!m.sync()) return;
         }
         L++;
@@ -466,6 +689,7 @@ __device__ __forceinline__ void sssp_body(const TravParams &p, Mode &m, uint32_t
         const unsigned slot = I % 3, nslot = (I + 1) % 3, rslot = (I + 2) % 3;
         const unsigned n_near = m.ld(u32_of(ctl->qlen[slot]));
         if (tid == 0) {
+            trace_iter(I, n_near | ((unsigned long long)m.ld(u32_of(ctl->far_len[P % 3])) << 32));
             *u32_of(ctl->qlen[rslot]) = 0;
             *u32_of(ctl->claim[rslot]) = 0;
             ctl->hub[rslot].v = 0;
@@ -482,7 +706,7 @@ __device__ __forceinline__ void sssp_body(const TravParams &p, Mode &m, uint32_t
             vis.fq.queue = sel2(p.far, P);
             vis.fq.len = u32_of(ctl->far_len[P % 3]);
             expand_frontier<SsspVisitor, SsspOwn>(vis, p, sel2(p.q, I), n_near, u32_of(ctl->claim[slot]),
-                                                  &ctl->hub[slot].v, pick_grain(n_near, nwarps), gwarp, nwarps, lane);
+                                                  &ctl->hub[slot].v, pick_grain(n_near, nwarps, p.uniform), gwarp, nwarps, lane);
             vis.nq.flush(lane);
             vis.fq.flush(lane);
             unsigned fm = warp_min_u32(vis.far_min);
@@ -516,7 +740,7 @@ __device__ __forceinline__ void sssp_body(const TravParams &p, Mode &m, uint32_t
             vis.fq.len = u32_of(ctl->far_len[(P + 1) % 3]);
             const uint32_t *pile = sel2(p.far, P);
             unsigned local_min = kInf;
-            const unsigned sgrain = pick_grain(nf, nwarps);
+            const unsigned sgrain = pick_grain(nf, nwarps, p.uniform);
             const ChunkSched cs{(nf + sgrain - 1) / sgrain, nwarps, gwarp, lane, u32_of(ctl->claim[slot])};
             for (unsigned c = cs.first(); c < cs.nchunks; c = cs.next()) {
                 const unsigned base = c * sgrain;

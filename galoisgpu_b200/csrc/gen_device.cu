@@ -182,6 +182,7 @@ extern "C" gft_status gft_graph_generate(int device, const gft_gen_params *p, vo
         if (err == cudaSuccess) {
             g = new gft_graph();
             g->g.device = device;
+            g->g.symmetric = true;  // every generator emits both directions of each edge
             g->g.nnodes = s.nnodes;
             g->g.nedges = (uint32_t)ne;
             err = cudaMalloc(&g->g.row_start, ((size_t)s.nnodes + 1) * 4);
@@ -202,6 +203,7 @@ extern "C" gft_status gft_graph_generate(int device, const gft_gen_params *p, vo
     if (err != cudaSuccess)
         st = fail(err == cudaErrorMemoryAllocation ? GFT_ERR_OOM : GFT_ERR_CUDA, "gft_graph_generate: %s",
                   cudaGetErrorString(err));
+    if (st == GFT_OK && g) st = graph_degree_stats(g->g, stream);
     cudaFree(k0);
     cudaFree(k1);
     cudaFree(d_nsel);

@@ -42,6 +42,8 @@ struct DeviceGraph {
     uint32_t *edge_dst = nullptr;
     int32_t *edge_data = nullptr;
     bool wrapped = false;
+    bool symmetric = false;  // every out-edge is also an in-edge: BFS may run bottom-up
+    uint32_t max_degree = 0;  // largest out-degree (set when the graph is created)
 };
 
 // Lazily grown device allocation owned by an engine.
@@ -100,7 +102,7 @@ struct BatchJob {
     uint32_t app;  // 0 BFS, 1 SSSP
     uint32_t hub_cap;
     uint32_t vec_ok;
-    uint32_t pad;
+    uint32_t uniform;  // max degree <= kUniformDegree: static chunks
     uint32_t status, error_where, levels, iterations;
     unsigned long long edges;
     unsigned long long t_start, t_end;  // %globaltimer, ns
@@ -135,6 +137,13 @@ namespace gft {
 // Resolves tuning defaults and the cooperative grid for a kernel.
 gft_status resolve_shape(gft_engine *e, const void *kernel, int block_threads, int blocks_per_sm,
                          size_t dyn_smem, LaunchShape *out);
+// Largest out-degree of a device graph, stored in G.max_degree (one small
+// reduction kernel on `stream`, then a wait).
+gft_status graph_degree_stats(DeviceGraph &G, cudaStream_t stream);
+// Graphs whose out-degrees are all at most this many edges have near-equal
+// work per frontier vertex, so a frontier is split into one static chunk
+// per warp (no shared claim cursor); others are claimed dynamically.
+constexpr uint32_t kUniformDegree = 32;
 gft_status check_engine_graph(gft_engine *e, const gft_graph *g);
 // Runs one BFS (is_sssp false) or SSSP query; caller holds e->mu.
 gft_status run_traversal(bool is_sssp, gft_engine *e, const gft_graph *g, uint32_t src, int32_t delta, int32_t *d_out,

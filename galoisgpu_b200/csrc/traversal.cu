@@ -37,7 +37,7 @@ namespace dev {
 template <int BLOCK>
 __global__ void __launch_bounds__(BLOCK, 2048 / BLOCK) bfs_persistent(TravParams p)
 {
-    __shared__ uint32_t s_buf[BLOCK / 32][64];
+    __shared__ uint32_t s_buf[BLOCK / 32][kQueueBuf];
     if ((int)blockIdx.x == p.skip_block) return;  // test hook: this CTA never arrives
     TraversalCtl *ctl = p.ctl;
     const unsigned tid = blockIdx.x * BLOCK + threadIdx.x, nthreads = gridDim.x * BLOCK;
@@ -49,8 +49,8 @@ __global__ void __launch_bounds__(BLOCK, 2048 / BLOCK) bfs_persistent(TravParams
 template <int BLOCK>
 __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) sssp_persistent(TravParams p)
 {
-    __shared__ uint32_t s_near[BLOCK / 32][64];
-    __shared__ uint32_t s_far[BLOCK / 32][64];
+    __shared__ uint32_t s_near[BLOCK / 32][kQueueBuf];
+    __shared__ uint32_t s_far[BLOCK / 32][kQueueBuf];
     if ((int)blockIdx.x == p.skip_block) return;
     TraversalCtl *ctl = p.ctl;
     const unsigned tid = blockIdx.x * BLOCK + threadIdx.x, nthreads = gridDim.x * BLOCK;
@@ -140,12 +140,13 @@ struct Tune {
     uint32_t block, bps, hub, timeout_ms;
     int skip;
     uint32_t max_blocks;
+    uint32_t direction;
 };
 
 Tune resolve_tuning(const gft_tuning *t, bool is_sssp)
 {
     Tune r{is_sssp ? kDefaultBlockSssp : kDefaultBlockBfs, kDefaultBlocksPerSm, kDefaultHubDegree, kDefaultTimeoutMs,
-           -1, 0};
+           -1, 0, 0};
     if (t) {
         if (t->block_threads) r.block = t->block_threads;
         if (t->blocks_per_sm) r.bps = t->blocks_per_sm;
@@ -153,6 +154,7 @@ Tune resolve_tuning(const gft_tuning *t, bool is_sssp)
         if (t->timeout_ms) r.timeout_ms = t->timeout_ms;
         r.skip = t->test_skip_block;
         r.max_blocks = t->max_blocks;
+        r.direction = t->direction;
     }
     return r;
 }
@@ -255,6 +257,9 @@ gft_status run_traversal(bool is_sssp, gft_engine *e, const gft_graph *g, uint32
     p.timeout_ns = (unsigned long long)t.timeout_ms * 1000000ull;
     p.skip_block = t.skip;
     p.vec_ok = ((uintptr_t)G.edge_dst % 16 == 0) && (!G.edge_data || (uintptr_t)G.edge_data % 16 == 0);
+    p.nedges = G.nedges;
+    p.dir_opt = !is_sssp && G.symmetric && t.direction == 0;
+    p.uniform = G.max_degree <= kUniformDegree;
 
     GFT_CUDA_TRY(cudaMemsetAsync(e->ctl.ptr, 0, sizeof(TraversalCtl), stream));
     void *args[] = {&p};
@@ -477,3 +482,11 @@ extern "C" gft_status gft_bfs_noalloc(const gft_graph *g, uint32_t src, int32_t 
     }
     return GFT_OK;
 }
+
+#ifdef GFT_TRACE
+extern "C" GFT_API int gft_debug_trace(unsigned long long *host, int max_records)
+{
+    const int n = max_records < 8192 ? max_records : 8192;
+    return cudaMemcpyFromSymbol(host, gft::dev::g_trace, sizeof(unsigned long long) * 2 * n) == cudaSuccess ? n : -1;
+}
+#endif

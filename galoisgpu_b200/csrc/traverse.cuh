@@ -140,27 +140,40 @@ struct GridSync {
     }
 };
 
-// Warp-aggregated append to a global queue through a 64-entry per-warp
-// shared-memory buffer.  `count` is warp uniform.  All 32 lanes must call
-// push() and flush() together.
+// Entries of each warp's shared-memory push buffer (a multiple of 32, at
+// least 64).  A larger buffer means fewer reservations on the queue's one
+// length counter, whose atomics serialise in a single L2 slice.
+#ifndef GFT_QBUF
+#define GFT_QBUF 128
+#endif
+constexpr unsigned kQueueBuf = GFT_QBUF;
+static_assert(kQueueBuf >= 64 && kQueueBuf % 32 == 0, "queue buffer: a multiple of 32, at least 64");
+
+// Warp-aggregated append to a global queue through a kQueueBuf-entry
+// per-warp shared-memory buffer: one atomic reservation per flush.  `count`
+// is warp uniform.  All 32 lanes must call push() and flush() together.
 struct WarpQueue {
-    uint32_t *buf;       // this warp's 64 shared-memory slots
+    uint32_t *buf;       // this warp's kQueueBuf shared-memory slots
     unsigned count;
     uint32_t *queue;     // global destination
     unsigned *len;       // global length counter
     unsigned cap;        // capacity of `queue`
     unsigned *err, *err_where;
 
-    __device__ __forceinline__ void store32(unsigned lane, unsigned n)
+    __device__ __forceinline__ void flush(unsigned lane)
     {
+        if (count == 0) return;
+        __syncwarp();
         unsigned base = 0;
-        if (lane == 0) base = atomicAdd(len, n);
+        if (lane == 0) base = atomicAdd(len, count);
         base = __shfl_sync(kFull, base, 0);
-        if (base + n > cap) {
+        if (base + count > cap) {
             if (lane == 0) raise_error(err, err_where, GFT_ERR_OVERFLOW, base);
-        } else if (lane < n) {
-            queue[base + lane] = buf[lane];
+        } else {
+            for (unsigned i = lane; i < count; i += 32) queue[base + i] = buf[i];
         }
+        __syncwarp();
+        count = 0;
     }
 
     __device__ __forceinline__ void push(bool p, uint32_t item, unsigned lane)
@@ -169,25 +182,7 @@ struct WarpQueue {
         if (mask == 0) return;
         if (p) buf[count + __popc(mask & lanemask_lt())] = item;
         count += __popc(mask);
-        if (count >= 32) {
-            __syncwarp();
-            store32(lane, 32);
-            unsigned rest = count - 32;
-            uint32_t x = lane < rest ? buf[32 + lane] : 0u;
-            __syncwarp();
-            if (lane < rest) buf[lane] = x;
-            __syncwarp();
-            count = rest;
-        }
-    }
-
-    __device__ __forceinline__ void flush(unsigned lane)
-    {
-        if (count == 0) return;
-        __syncwarp();
-        store32(lane, count);
-        __syncwarp();
-        count = 0;
+        if (count > kQueueBuf - 32) flush(lane);
     }
 };
 
@@ -227,6 +222,14 @@ __device__ __forceinline__ void warp_flatten(uint32_t start, uint32_t deg, unsig
 
 // Block-wide sum of a 64-bit value into *dst (one atomic per warp).
 __device__ __forceinline__ void warp_add_u64(unsigned long long *dst, unsigned long long v, unsigned lane)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(kFull, v, o);
+    if (lane == 0 && v) atomicAdd(dst, v);
+}
+
+// Warp-wide sum of a 32-bit value into *dst (one atomic per warp).
+__device__ __forceinline__ void warp_add_u32(unsigned *dst, unsigned v, unsigned lane)
 {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(kFull, v, o);

@@ -131,21 +131,30 @@ class CSRGraph:
     def grid(cls, rows: int, cols: int, seed: int = 0, max_weight: int = 1) -> "CSRGraph":
         csr = Csr()
         check(load().gft_gen_grid(rows, cols, seed, max_weight, C.byref(csr)))
-        return cls(*_take_csr(csr))
+        return cls(*_take_csr(csr))._mark_symmetric()
 
     @classmethod
     def road(cls, side: int, seed: int = 1, delete_ppm: int = 50000, shortcut_ppm: int = 1000,
              max_weight: int = 10000) -> "CSRGraph":
         csr = Csr()
         check(load().gft_gen_road(side, seed, delete_ppm, shortcut_ppm, max_weight, C.byref(csr)))
-        return cls(*_take_csr(csr))
+        return cls(*_take_csr(csr))._mark_symmetric()
 
     @classmethod
     def rmat(cls, scale: int, edge_factor: int = 16, seed: int = 1, max_weight: int = 0,
              a: int = RMAT_A, b: int = RMAT_B, c: int = RMAT_C) -> "CSRGraph":
         csr = Csr()
         check(load().gft_gen_rmat(scale, edge_factor, a, b, c, seed, max_weight, C.byref(csr)))
-        return cls(*_take_csr(csr))
+        return cls(*_take_csr(csr))._mark_symmetric()
+
+    # The generators emit both directions of every edge.  A graph read from
+    # a file or built from arrays is marked only by the caller (symmetric =
+    # True), and only when every edge u->v has v->u.
+    symmetric = False
+
+    def _mark_symmetric(self) -> "CSRGraph":
+        self.symmetric = True
+        return self
 
     def pick_sources(self, seed: int, k: int) -> list[int]:
         out = (C.c_uint32 * k)()
@@ -157,7 +166,10 @@ class CSRGraph:
         c = self._csr()
         h = C.c_void_p()
         check(load().gft_graph_upload(device, C.byref(c), _stream_ptr(stream), C.byref(h)))
-        return DeviceGraph(h, device)
+        d = DeviceGraph(h, device)
+        if self.symmetric:
+            d.symmetric = True
+        return d
 
 
 def _stream_ptr(stream) -> C.c_void_p:
@@ -209,6 +221,17 @@ class DeviceGraph:
             raise ValueError("graph was freed")
         return self._h
 
+    @property
+    def symmetric(self) -> bool:
+        """Whether BFS may run bottom-up levels (gft_graph_set_symmetric)."""
+        v = C.c_int()
+        check(load().gft_graph_is_symmetric(self.handle, C.byref(v)))
+        return bool(v.value)
+
+    @symmetric.setter
+    def symmetric(self, value: bool) -> None:
+        check(load().gft_graph_set_symmetric(self.handle, 1 if value else 0))
+
     def arrays(self) -> tuple[int, int, int]:
         rs, dst, w = C.c_void_p(), C.c_void_p(), C.c_void_p()
         check(load().gft_graph_arrays(self.handle, C.byref(rs), C.byref(dst), C.byref(w)))
@@ -249,10 +272,11 @@ class Tune:
     max_blocks: int = 0
     group_blocks: int = 0
     group_min_nodes: int = 0
+    direction: int = 0  # BFS: 0 = direction-optimising on graphs marked symmetric, 1 = top-down only
 
     def c(self) -> Tuning:
         return Tuning(self.block_threads, self.blocks_per_sm, self.hub_degree, self.timeout_ms, self.test_skip_block,
-                      self.max_blocks, self.group_blocks, self.group_min_nodes)
+                      self.max_blocks, self.group_blocks, self.group_min_nodes, self.direction)
 
 
 class Engine:

@@ -92,6 +92,8 @@ typedef struct gft_tuning {
     uint32_t group_min_nodes; /* batches: queries on graphs with at least this many
                                  vertices run on a CTA group (0 = 262144; set it
                                  above every graph to run each query on one CTA) */
+    uint32_t direction;       /* BFS: 0 = direction-optimising when the graph is
+                                 marked symmetric, 1 = top-down only          */
 } gft_tuning;
 
 /* ---------------------------------------------------------------------------
@@ -164,6 +166,15 @@ typedef struct gft_gen_params {
 } gft_gen_params;
 GFT_API gft_status gft_graph_generate(int device, const gft_gen_params *p, void *stream, gft_graph **out);
 GFT_API gft_status gft_graph_info(const gft_graph *g, uint32_t *nnodes, uint32_t *nedges, int *weighted);
+/* Symmetry mark (no counterpart in the reference, whose BFS is top-down
+ * only).  A graph marked symmetric (every edge u->v has v->u) lets gft_bfs
+ * run direction-optimising: levels with a large frontier run bottom-up,
+ * each unvisited vertex looking for a parent among its own edges.
+ * gft_graph_generate marks its graphs; uploaded and wrapped graphs start
+ * unmarked, and the caller marks them only when the mark is true (a wrong
+ * mark gives wrong levels).  Levels are the same in either direction. */
+GFT_API gft_status gft_graph_set_symmetric(gft_graph *g, int symmetric);
+GFT_API gft_status gft_graph_is_symmetric(const gft_graph *g, int *symmetric);
 /* Device pointers of a graph (any may be NULL). */
 GFT_API gft_status gft_graph_arrays(const gft_graph *g, const uint32_t **d_row_start, const uint32_t **d_edge_dst,
                             const int32_t **d_edge_data);

@@ -162,3 +162,76 @@ def test_invalid_arguments(gft, engine):
         engine.sssp(dg, 0, delta=0)
     with pytest.raises(gft.GftError, match="INVALID_ARG"):
         engine.bfs(dg, 0, tune=gft.Tune(block_threads=300))
+
+
+@pytest.mark.parametrize("tune", TUNES, ids=["default", "256x4", "1024x1", "hub32"])
+def test_direction_optimising_bfs(gft, orc, engine, tune):
+    """On a graph marked symmetric, BFS runs bottom-up levels when the
+    frontier is large: levels equal the oracle's and the top-down-only run's,
+    parents form a valid BFS tree, and far fewer edges are examined."""
+    g = gft.CSRGraph.rmat(17, 16, seed=11)
+    assert g.symmetric
+    dg = g.copy_to_gpu()
+    assert dg.symmetric
+    for src in g.pick_sources(4, 3):
+        want = orc.bfs(g.row_start, g.edge_dst, src)
+        got, par, r = _run_bfs(gft, engine, dg, src, tune)
+        np.testing.assert_array_equal(got, want)
+        assert orc.check_tree(g.row_start, g.edge_dst, None, src, got, par) == 0
+        td, _, r_td = _run_bfs(gft, engine, dg, src, {**tune, "direction": 1})
+        np.testing.assert_array_equal(td, want)
+        assert r["edges_scanned"] < r_td["edges_scanned"] / 2
+
+
+def test_direction_optimising_needs_the_symmetry_mark(gft, orc, engine):
+    """A directed graph is never traversed bottom-up: an unmarked upload stays
+    top-down, and the mark is the caller's to set."""
+    rs = np.array([0, 1, 2, 3, 3], dtype=np.uint32)  # 0 -> 1 -> 2 -> 3, one way
+    dst = np.array([1, 2, 3], dtype=np.uint32)
+    g = gft.CSRGraph(rs, dst, None)
+    assert not g.symmetric
+    dg = g.copy_to_gpu()
+    assert not dg.symmetric
+    for src in range(4):
+        got, par, _ = _run_bfs(gft, engine, dg, src)
+        np.testing.assert_array_equal(got, orc.bfs(rs, dst, src))
+    dg.symmetric = True
+    assert dg.symmetric
+
+
+def test_grid_and_road_bfs_with_static_chunks(gft, orc, engine):
+    """Low-degree graphs split large frontiers into one static chunk per
+    warp; levels and parents stay exact."""
+    for g in (gft.CSRGraph.grid(700, 700, 0, 1), gft.CSRGraph.road(600, seed=4)):
+        dg = g.copy_to_gpu()
+        for src in g.pick_sources(9, 2):
+            got, par, _ = _run_bfs(gft, engine, dg, src)
+            np.testing.assert_array_equal(got, orc.bfs(g.row_start, g.edge_dst, src))
+            assert orc.check_tree(g.row_start, g.edge_dst, None, src, got, par) == 0
+
+
+def test_direction_optimising_on_a_uniform_low_diameter_graph(gft, orc, engine):
+    """A random graph of small, even degree takes the uniform-degree path of
+    the direction switch (no degree loads) and still runs bottom-up."""
+    rng = np.random.default_rng(5)
+    n, m = 200_000, 800_000
+    u = rng.integers(0, n, m, dtype=np.int64)
+    v = rng.integers(0, n, m, dtype=np.int64)
+    keep = u != v
+    a = np.concatenate([u[keep], v[keep]])
+    b = np.concatenate([v[keep], u[keep]])
+    key = np.unique(a * n + b)
+    src_of, dst = (key // n).astype(np.uint32), (key % n).astype(np.uint32)
+    rs = np.zeros(n + 1, dtype=np.uint32)
+    np.cumsum(np.bincount(src_of, minlength=n), out=rs[1:])
+    g = gft.CSRGraph(rs, dst, None)
+    assert int(np.diff(rs.astype(np.int64)).max()) <= 32
+    dg = g.copy_to_gpu()
+    dg.symmetric = True
+    for src in g.pick_sources(3, 2):
+        want = orc.bfs(rs, dst, src)
+        got, par, r = _run_bfs(gft, engine, dg, src)
+        np.testing.assert_array_equal(got, want)
+        assert orc.check_tree(rs, dst, None, src, got, par) == 0
+        _, _, r_td = _run_bfs(gft, engine, dg, src, {"direction": 1})
+        assert r["edges_scanned"] < r_td["edges_scanned"]
