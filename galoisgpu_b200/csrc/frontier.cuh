@@ -207,8 +207,13 @@ struct SsspVisitor {
                                            const SsspOwn (&o)[K], unsigned lane)
     {
         unsigned long long cur[K];
+#ifdef GFT_NO_PRECHECK
+#pragma unroll
+        for (int k = 0; k < K; k++) cur[k] = ~0ull;
+#else
 #pragma unroll
         for (int k = 0; k < K; k++) cur[k] = valid[k] ? __ldcg(dt + v[k]) : 0ull;
+#endif
         uint32_t nd[K];
         bool to_near[K], to_far[K];
 #pragma unroll
@@ -527,7 +532,7 @@ struct CtaMode {
 // Direction switch (Beamer et al.): go bottom-up once the frontier's edges
 // exceed 1/kAlpha of the edges still unexplored, and back top-down once the
 // frontier holds fewer than 1/kBeta of the vertices.
-constexpr unsigned kAlpha = 14, kBeta = 24;
+constexpr unsigned kAlpha = 14, kBeta = 24, kScan = 32;
 
 template <class Mode>
 __device__ __forceinline__ void bfs_body(const TravParams &p, Mode &m, uint32_t *warp_buf)
@@ -576,6 +581,7 @@ __device__ __forceinline__ void bfs_body(const TravParams &p, Mode &m, uint32_t 
     bool bottom_up = false;
     unsigned long long m_seen = 0;  // out-degree sum of the frontiers of finished levels
     unsigned long long n_seen = 0;  // vertices reached so far (uniform-degree estimate)
+    unsigned n_prev = 0;            // previous frontier size
     for (;;) {
         const unsigned slot = L % 3, nslot = (L + 1) % 3, rslot = (L + 2) % 3;
         const unsigned n_in = m.ld(u32_of(ctl->qlen[slot]));
@@ -595,8 +601,17 @@ __device__ __forceinline__ void bfs_body(const TravParams &p, Mode &m, uint32_t 
                 m_u = E - min(E, m_seen + mf);
                 m_seen += mf;
             }
-            bottom_up = bottom_up ? (unsigned long long)n_in * kBeta >= n : mf * kAlpha > m_u;
+            // A bottom-up level also pays a pass over the visited bitmap (one
+            // word per 32 vertices), so the switch charges n / kScan edge
+            // equivalents for it; and it needs a growing frontier.  On a
+            // high-diameter graph the frontier stops growing long before the
+            // unexplored edges run low, and most unvisited vertices are far
+            // from it and would scan all their edges in vain, so its
+            // traversal stays top-down.
+            bottom_up = bottom_up ? (unsigned long long)n_in * kBeta >= n
+                                  : n_in > n_prev && mf > m_u / kAlpha + n / kScan;
         }
+        n_prev = n_in;
         if (tid == 0) {
             trace_iter(L, n_in | ((unsigned long long)bottom_up << 32));
             *u32_of(ctl->qlen[rslot]) = 0;

@@ -64,6 +64,12 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) msbfs_kernel(MsParams p)
     GridSync gs{&ctl->barrier.v, u32_of(ctl->release), &ctl->error, &ctl->error_where, gridDim.x, 0, p.timeout_ns};
     const uint32_t n = p.nnodes, W = p.words;
     const size_t plane_words = (size_t)n * W;
+    // Warp-aggregated appends (one reservation per flush) for the next
+    // frontier and the top-down touched list.
+    __shared__ uint32_t s_next[BLOCK / 32][kQueueBuf];
+    __shared__ uint32_t s_touch[BLOCK / 32][kQueueBuf];
+    WarpQueue nq{s_next[threadIdx.x >> 5], 0, nullptr, nullptr, n, &ctl->error, &ctl->error_where};
+    WarpQueue tq{s_touch[threadIdx.x >> 5], 0, p.touched, nullptr, n, &ctl->error, &ctl->error_where};
     // counters: qlen[slot] frontier size, claim[slot] touched count,
     // hub[slot].v frontier edge count m_f.
 
@@ -115,6 +121,9 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) msbfs_kernel(MsParams p)
         uint32_t *qn = p.queue[(L + 1) & 1];
         unsigned *qn_len = u32_of(ctl->qlen[nslot]);
         unsigned long long *mf_next = &ctl->hub[nslot].v;
+        nq.queue = qn;
+        nq.len = qn_len;
+        tq.len = u32_of(ctl->claim[slot]);
         unsigned long long my_mf = 0;
         const bool bottom_up = p.symmetric && mf * p.alpha > p.nedges;
         if (bottom_up) {
@@ -166,10 +175,8 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) msbfs_kernel(MsParams p)
                 }
 #pragma unroll
                 for (int w = 0; w < kMaxWords; w++) got |= acc[w] != 0;
-                if (got && lane == 0) {
-                    qn[atomicAdd(qn_len, 1u)] = v;
-                    my_mf += e - s;
-                }
+                if (got && lane == 0) my_mf += e - s;
+                nq.push(got && lane == 0, v, lane);
             }
         } else {
             // Top-down: clear the next plane, expand, commit.
@@ -182,45 +189,53 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) msbfs_kernel(MsParams p)
 #pragma unroll
                 for (int w = 0; w < kMaxWords; w++) fu[w] = w < (int)W ? __ldcg(F + (size_t)u * W + w) : 0u;
                 const uint32_t s = p.row_start[u], e = p.row_start[u + 1];
-                for (uint32_t ei = s + lane; ei < e; ei += 32) {
-                    const uint32_t v = __ldcs(p.edge_dst + ei);
-                    uint32_t *sv = row(p.seen, v, W), *nv = row(p.next, v, W);
+                for (uint32_t eb = s; eb < e; eb += 32) {  // warp-uniform trip count
+                    const uint32_t ei = eb + lane;
                     bool touched = false;
+                    uint32_t v = 0;
+                    if (ei < e) {
+                        v = __ldcs(p.edge_dst + ei);
+                        uint32_t *sv = row(p.seen, v, W), *nv = row(p.next, v, W);
 #pragma unroll
-                    for (int w = 0; w < kMaxWords; w++) {
-                        if (w < (int)W && fu[w]) {
-                            const uint32_t b = fu[w] & ~__ldcg(sv + w);
-                            if (b) {
-                                atomicOr(nv + w, b);
-                                touched = true;
+                        for (int w = 0; w < kMaxWords; w++) {
+                            if (w < (int)W && fu[w]) {
+                                const uint32_t b = fu[w] & ~__ldcg(sv + w);
+                                if (b) {
+                                    atomicOr(nv + w, b);
+                                    touched = true;
+                                }
                             }
                         }
+                        touched = touched && atomicExch(p.tstamp + v, L + 1) != L + 1;
                     }
-                    if (touched && atomicExch(p.tstamp + v, L + 1) != L + 1)
-                        p.touched[atomicAdd(u32_of(ctl->claim[slot]), 1u)] = v;
+                    tq.push(touched, v, lane);
                 }
             }
+            tq.flush(lane);
             if (!gs.sync()) return;
             const uint32_t nt = ld_relaxed_u32(u32_of(ctl->claim[slot]));
-            for (uint32_t ti = tid; ti < nt; ti += nthreads) {
-                const uint32_t v = __ldcg(p.touched + ti);
-                uint32_t *sv = row(p.seen, v, W), *nv = row(p.next, v, W), *fv = row(Fn, v, W);
+            for (uint32_t b = gwarp * 32; b < nt; b += nwarps * 32) {  // warp-uniform trip count
+                const uint32_t ti = b + lane;
                 bool got = false;
-                for (uint32_t w = 0; w < W; w++) {
-                    const uint32_t nb = __ldcg(nv + w) & ~__ldcg(sv + w);
-                    nv[w] = 0;
-                    if (nb) {
-                        fv[w] = nb;
-                        sv[w] |= nb;
-                        got = true;
+                uint32_t v = 0;
+                if (ti < nt) {
+                    v = __ldcg(p.touched + ti);
+                    uint32_t *sv = row(p.seen, v, W), *nv = row(p.next, v, W), *fv = row(Fn, v, W);
+                    for (uint32_t w = 0; w < W; w++) {
+                        const uint32_t nb = __ldcg(nv + w) & ~__ldcg(sv + w);
+                        nv[w] = 0;
+                        if (nb) {
+                            fv[w] = nb;
+                            sv[w] |= nb;
+                            got = true;
+                        }
                     }
+                    if (got) my_mf += p.row_start[v + 1] - p.row_start[v];
                 }
-                if (got) {
-                    qn[atomicAdd(qn_len, 1u)] = v;
-                    my_mf += p.row_start[v + 1] - p.row_start[v];
-                }
+                nq.push(got, v, lane);
             }
         }
+        nq.flush(lane);
         warp_add_u64(mf_next, my_mf, lane);
         if (!gs.sync()) return;
         L++;

@@ -31,6 +31,8 @@
 namespace gft {
 namespace dev {
 
+constexpr int kCtaBlock = 1024;  // threads of the single-CTA kernels
+
 // ---------------------------------------------------------------------------
 // Single-query kernels: the whole cooperative grid is one group.
 // ---------------------------------------------------------------------------
@@ -57,6 +59,57 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) sssp_persistent(TravParam
     GridMode m{{&ctl->barrier.v, u32_of(ctl->release), &ctl->error, &ctl->error_where, gridDim.x, 0, p.timeout_ns},
                ctl, tid, nthreads, tid / 32, nthreads / 32};
     sssp_body(p, m, s_near[threadIdx.x >> 5], s_far[threadIdx.x >> 5]);
+}
+
+// ---------------------------------------------------------------------------
+// Single-CTA kernels for small graphs.  A small graph's frontiers are small
+// and its levels many (the 256^2 grid: 511 levels of at most 512 vertices),
+// so a grid barrier per level dominates.  One CTA runs the whole traversal
+// with its control block in shared memory and __syncthreads as the barrier
+// (CtaMode, as the batched kernel's small jobs), then copies the results to
+// the engine's control block.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void publish_cta_result(const TraversalCtl &s, TraversalCtl *g)
+{
+    g->error = s.error;
+    g->error_where = s.error_where;
+    g->levels = s.levels;
+    g->iterations = s.iterations;
+    g->threshold = s.threshold;
+    g->edges = s.edges;
+    g->pushes = s.pushes;
+    g->reached = s.reached;
+}
+
+__global__ void __launch_bounds__(kCtaBlock, 1) bfs_single_cta(TravParams p)
+{
+    __shared__ TraversalCtl s_ctl;
+    __shared__ uint32_t s_buf[kCtaBlock / 32][kQueueBuf];
+    for (unsigned i = threadIdx.x; i < sizeof(TraversalCtl) / 4; i += kCtaBlock)
+        reinterpret_cast<unsigned *>(&s_ctl)[i] = 0;
+    __syncthreads();
+    TraversalCtl *gctl = p.ctl;
+    p.ctl = &s_ctl;
+    CtaMode m{&s_ctl, threadIdx.x, kCtaBlock, threadIdx.x >> 5, kCtaBlock / 32, 0};
+    bfs_body(p, m, s_buf[threadIdx.x >> 5]);
+    __syncthreads();
+    if (threadIdx.x == 0) publish_cta_result(s_ctl, gctl);
+}
+
+__global__ void __launch_bounds__(kCtaBlock, 1) sssp_single_cta(TravParams p)
+{
+    __shared__ TraversalCtl s_ctl;
+    __shared__ uint32_t s_near[kCtaBlock / 32][kQueueBuf];
+    __shared__ uint32_t s_far[kCtaBlock / 32][kQueueBuf];
+    for (unsigned i = threadIdx.x; i < sizeof(TraversalCtl) / 4; i += kCtaBlock)
+        reinterpret_cast<unsigned *>(&s_ctl)[i] = 0;
+    __syncthreads();
+    TraversalCtl *gctl = p.ctl;
+    p.ctl = &s_ctl;
+    CtaMode m{&s_ctl, threadIdx.x, kCtaBlock, threadIdx.x >> 5, kCtaBlock / 32, 0};
+    sssp_body(p, m, s_near[threadIdx.x >> 5], s_far[threadIdx.x >> 5]);
+    __syncthreads();
+    if (threadIdx.x == 0) publish_cta_result(s_ctl, gctl);
 }
 
 // SSSP parent tree from final distances: parent[v] = some u with
@@ -115,6 +168,11 @@ constexpr uint32_t kDefaultBlockSssp = 512;
 constexpr uint32_t kDefaultBlocksPerSm = 2;
 constexpr uint32_t kDefaultHubDegree = 256;
 constexpr uint32_t kDefaultTimeoutMs = 20000;
+// Graphs up to this size run on one CTA by default: their frontiers are
+// small enough for 1024 threads, and a __syncthreads per level is several
+// times cheaper than a grid barrier (BFS on the 256^2 grid: 511 levels).
+constexpr uint32_t kCtaMaxNodes = 1u << 17;
+constexpr uint32_t kCtaMaxEdges = 1u << 19;
 
 const void *bfs_kernel_for(int block)
 {
@@ -202,9 +260,21 @@ gft_status run_traversal(bool is_sssp, gft_engine *e, const gft_graph *g, uint32
     if (!kern) return fail(GFT_ERR_INVALID_ARG, "%s: block_threads must be 256, 512 or 1024", what);
     if (t.hub < 32) t.hub = 32;
     GFT_CUDA_TRY(cudaSetDevice(e->device));
+    // One CTA for small graphs (max_blocks 0 = automatic) or on request
+    // (max_blocks 1); the whole cooperative grid otherwise.
+    const bool single = t.max_blocks == 1 || (t.max_blocks == 0 && t.skip < 0 && G.nnodes <= kCtaMaxNodes &&
+                                              G.nedges <= kCtaMaxEdges);
     LaunchShape shape;
-    GFT_TRY(resolve_shape(e, kern, (int)t.block, (int)t.bps, 0, &shape));
-    if (t.max_blocks && (uint32_t)shape.blocks > t.max_blocks) shape.blocks = (int)t.max_blocks;
+    if (single) {
+        shape.block_threads = dev::kCtaBlock;
+        shape.blocks = 1;
+        shape.blocks_per_sm = 1;
+        shape.sms = e->sms;
+        kern = is_sssp ? (const void *)dev::sssp_single_cta : (const void *)dev::bfs_single_cta;
+    } else {
+        GFT_TRY(resolve_shape(e, kern, (int)t.block, (int)t.bps, 0, &shape));
+        if (t.max_blocks && (uint32_t)shape.blocks > t.max_blocks) shape.blocks = (int)t.max_blocks;
+    }
 
     // Scratch layout.
     const uint32_t n = G.nnodes;
@@ -264,7 +334,10 @@ gft_status run_traversal(bool is_sssp, gft_engine *e, const gft_graph *g, uint32
     GFT_CUDA_TRY(cudaMemsetAsync(e->ctl.ptr, 0, sizeof(TraversalCtl), stream));
     void *args[] = {&p};
     GFT_CUDA_TRY(cudaEventRecord(e->ev0, stream));
-    GFT_CUDA_TRY(cudaLaunchCooperativeKernel(kern, dim3(shape.blocks), dim3(shape.block_threads), args, 0, stream));
+    if (single)
+        GFT_CUDA_TRY(cudaLaunchKernel(kern, dim3(1), dim3(shape.block_threads), args, 0, stream));
+    else
+        GFT_CUDA_TRY(cudaLaunchCooperativeKernel(kern, dim3(shape.blocks), dim3(shape.block_threads), args, 0, stream));
     GFT_CUDA_TRY(cudaEventRecord(e->ev1, stream));
     if (is_sssp && d_parent) {
         dev::parent_init<<<e->sms * 4, 256, 0, stream>>>(d_parent, n, src);

@@ -87,7 +87,9 @@ typedef struct gft_tuning {
     uint32_t hub_degree;      /* degree at which a vertex is split across the grid  */
     uint32_t timeout_ms;      /* bound on every device-side wait                    */
     int32_t test_skip_block;  /* test hook: CTA that never arrives (-1 = none)      */
-    uint32_t max_blocks;      /* cap on the persistent grid (0 = no cap)            */
+    uint32_t max_blocks;      /* cap on the persistent grid; 0 = automatic (graphs
+                                 of <= 2^17 vertices and <= 2^19 edges run on one
+                                 CTA, larger ones on the whole grid); 1 = one CTA */
     uint32_t group_blocks;    /* batches: CTAs that share one large query (0 = 8)   */
     uint32_t group_min_nodes; /* batches: queries on graphs with at least this many
                                  vertices run on a CTA group (0 = 262144; set it

@@ -10,11 +10,13 @@ from graphs import hand_cases
 pytestmark = pytest.mark.gpu
 
 TUNES = [
-    dict(),
-    dict(block_threads=256, blocks_per_sm=4),
-    dict(block_threads=1024, blocks_per_sm=1),
-    dict(hub_degree=32),  # every vertex of degree >= 32 goes through the grid-wide hub phase
+    dict(),  # small graphs run on one CTA, larger ones on the whole grid
+    dict(block_threads=256, blocks_per_sm=4, max_blocks=1 << 30),  # always the grid
+    dict(block_threads=1024, blocks_per_sm=1, max_blocks=1 << 30),
+    dict(hub_degree=32, max_blocks=1 << 30),  # every vertex of degree >= 32 goes through the grid-wide hub phase
+    dict(max_blocks=1, hub_degree=32),  # always one CTA
 ]
+TUNE_IDS = ["auto", "grid256x4", "grid1024x1", "grid-hub32", "one-cta"]
 
 
 def _sources(n):
@@ -164,7 +166,7 @@ def test_invalid_arguments(gft, engine):
         engine.bfs(dg, 0, tune=gft.Tune(block_threads=300))
 
 
-@pytest.mark.parametrize("tune", TUNES, ids=["default", "256x4", "1024x1", "hub32"])
+@pytest.mark.parametrize("tune", TUNES, ids=TUNE_IDS)
 def test_direction_optimising_bfs(gft, orc, engine, tune):
     """On a graph marked symmetric, BFS runs bottom-up levels when the
     frontier is large: levels equal the oracle's and the top-down-only run's,
