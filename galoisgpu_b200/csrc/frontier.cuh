@@ -579,9 +579,10 @@ __device__ __forceinline__ void bfs_body(const TravParams &p, Mode &m, uint32_t 
 
     unsigned L = 0;
     bool bottom_up = false;
-    unsigned long long m_seen = 0;  // out-degree sum of the frontiers of finished levels
+    unsigned long long m_seen = 0;  // out-degree sum of the frontiers reached so far
     unsigned long long n_seen = 0;  // vertices reached so far (uniform-degree estimate)
     unsigned n_prev = 0;            // previous frontier size
+    const float n_f = (float)n, E_f = (float)p.nedges, mean_deg = E_f / fmaxf(1.f, n_f);
     for (;;) {
         const unsigned slot = L % 3, nslot = (L + 1) % 3, rslot = (L + 2) % 3;
         const unsigned n_in = m.ld(u32_of(ctl->qlen[slot]));
@@ -590,26 +591,31 @@ __device__ __forceinline__ void bfs_body(const TravParams &p, Mode &m, uint32_t 
             break;
         }
         if (p.dir_opt) {  // every thread reads the same counters: a uniform decision
-            const unsigned long long E = p.nedges;
-            unsigned long long mf, m_u;
+            // Single-precision arithmetic: the switch is a heuristic, and
+            // 64-bit divisions by n would cost about a microsecond per level.
+            float mf, m_u;
             if (p.uniform) {
                 n_seen += n_in;
-                mf = (unsigned long long)n_in * E / n;
-                m_u = E - min(E, n_seen * E / n);
+                mf = (float)n_in * mean_deg;
+                m_u = fmaxf(0.f, E_f - (float)n_seen * mean_deg);
             } else {
-                mf = m.ld(u32_of(ctl->far_len[slot]));
-                m_u = E - min(E, m_seen + mf);
-                m_seen += mf;
+                const unsigned mfi = m.ld(u32_of(ctl->far_len[slot]));
+                m_seen += mfi;
+                mf = (float)mfi;
+                m_u = fmaxf(0.f, E_f - (float)m_seen);
             }
             // A bottom-up level also pays a pass over the visited bitmap (one
             // word per 32 vertices), so the switch charges n / kScan edge
             // equivalents for it; and it needs a growing frontier.  On a
             // high-diameter graph the frontier stops growing long before the
             // unexplored edges run low, and most unvisited vertices are far
-            // from it and would scan all their edges in vain, so its
-            // traversal stays top-down.
-            bottom_up = bottom_up ? (unsigned long long)n_in * kBeta >= n
-                                  : n_in > n_prev && mf > m_u / kAlpha + n / kScan;
+            // from it and would scan all their edges in vain.  A uniform-degree
+            // graph also needs a frontier of n / kBeta vertices: its frontier
+            // edges are an estimate, and a road network's frontier can wobble
+            // upward past its peak.
+            const bool big = (float)n_in * kBeta >= n_f;
+            bottom_up = bottom_up ? big
+                                  : n_in > n_prev && (big || !p.uniform) && mf > m_u / kAlpha + n_f / kScan;
         }
         n_prev = n_in;
         if (tid == 0) {
