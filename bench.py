@@ -568,8 +568,8 @@ def bench_msbfs(gft, dev: int, k: int = 256, reps: int = 3, max_levels: int = 16
     srcs = dg.pick_sources(spec["src_seed"], k)
     eng = gft.Engine(dev)
     tune, _, tune_desc = tuned_for(gft, "bfs-rmat-24", spec)
-    words = (k + 31) // 32
-    planes = torch.empty(max_levels * dg.nnodes * words, dtype=torch.int32, device=f"cuda:{dev}")
+    plane_bytes = gft.load().gft_msbfs_plane_bytes(dg.nnodes, k)
+    planes = torch.empty(max_levels * plane_bytes // 4, dtype=torch.int32, device=f"cuda:{dev}")
     r = eng.msbfs(dg, srcs, max_levels=max_levels, symmetric=True, planes=planes)  # warm-up
     ms = []
     for _ in range(reps):

@@ -353,10 +353,9 @@ class Engine:
         import torch
 
         k = len(sources)
-        words = (k + 31) // 32
+        plane = load().gft_msbfs_plane_bytes(graph.nnodes, k)
         if planes is None:
-            planes = torch.empty(max_levels * graph.nnodes * words, dtype=torch.int32,
-                                 device=f"cuda:{graph.device}")
+            planes = torch.empty(max_levels * plane // 4, dtype=torch.int32, device=f"cuda:{graph.device}")
         src = (C.c_uint32 * k)(*sources)
         st = Stats()
         dev = torch.device("cuda", graph.device)

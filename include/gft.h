@@ -359,9 +359,11 @@ GFT_API gft_status gft_serve_close(gft_server *s);
  * Multi-source BFS (no counterpart in the reference, which runs one source
  * per process).  k <= 256 BFS queries on one graph in one launch with
  * per-vertex bitsets (one bit per source).  The result is a stack of
- * frontier planes in caller memory: d_planes holds max_levels planes of
- * gft_msbfs_plane_bytes(nnodes, k) bytes each; plane L, vertex v, bit i is
- * set iff source i reaches v at level L.  stats->levels = planes used;
+ * frontier planes in caller memory (16-byte aligned): d_planes holds
+ * max_levels planes of gft_msbfs_plane_bytes(nnodes, k) bytes each.  A plane
+ * has one row of WP words per vertex, WP = ceil(k / 32) rounded up to 1, 2,
+ * 4 or 8; in plane L, bit i % 32 of word i / 32 of vertex v's row is set iff
+ * source i reaches v at level L.  stats->levels = planes used;
  * GFT_ERR_OVERFLOW if the traversal needs more than max_levels.
  * gft_msbfs_levels writes source i's int32 levels (as gft_bfs would) from
  * the planes.  flags: GFT_MSBFS_SYMMETRIC allows bottom-up levels (the
