@@ -140,6 +140,8 @@ class ServeConfig(C.Structure):
         ("sparse_degree", C.c_uint32),
         ("queue_capacity", C.c_uint32),
         ("max_lanes_per_request", C.c_uint32),
+        ("wide_lanes", C.c_uint32),
+        ("wide_min_edges", C.c_uint32),
     ]
 
 

@@ -56,6 +56,7 @@ __device__ __forceinline__ TravParams job_params(const BatchJob &jb, char *scrat
     p.vec_ok = jb.vec_ok;
     p.uniform = jb.uniform;
     p.nedges = jb.nedges;
+    p.dir_opt = jb.dir_opt;
     if (jb.app == 1) {
         p.far[0] = reinterpret_cast<uint32_t *>(base + 2 * qbytes);
         p.far[1] = reinterpret_cast<uint32_t *>(base + 3 * qbytes);
@@ -97,6 +98,11 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK)
     __shared__ uint32_t s_near[BLOCK / 32][kQueueBuf];
     __shared__ uint32_t s_far[BLOCK / 32][kQueueBuf];
     __shared__ unsigned s_job;
+    // The running job's parameters live in shared memory: the traversal
+    // bodies read them by reference, which keeps them out of registers.
+    __shared__ TravParams s_p;
+    __shared__ unsigned s_app;
+    __shared__ unsigned long long s_t0;
     const unsigned w = threadIdx.x >> 5;
 
     // Phase 1: large jobs on CTA groups.
@@ -129,13 +135,18 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK)
                 }
             }
             if (!gs.sync()) break;
-            const BatchJob jb = jobs[j];
-            const unsigned long long t0 = globaltimer_ns();
-            TravParams p = job_params(jb, scratch, hub_degree, ctl);
+            if (threadIdx.x == 0) {
+                const BatchJob jb = jobs[j];
+                s_p = job_params(jb, scratch, hub_degree, ctl);
+                s_app = jb.app;
+                s_t0 = globaltimer_ns();
+            }
+            __syncthreads();
+            const unsigned long long t0 = s_t0;
             const unsigned tid = rank * BLOCK + threadIdx.x;
             GridMode m{gs, ctl, tid, group * BLOCK, tid / 32, group * BLOCK / 32};
-            if (jb.app == 1) sssp_body(p, m, s_near[w], s_far[w]);
-            else bfs_body(p, m, s_near[w]);
+            if (s_app == 1) sssp_body(s_p, m, s_near[w], s_far[w]);
+            else bfs_body(s_p, m, s_near[w]);
             gs.epoch = m.gs.epoch;
             const bool ok = gs.sync();
             if (rank == 0 && threadIdx.x == 0) {
@@ -159,12 +170,17 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK)
         __syncthreads();
         const unsigned j = s_job;
         if (j >= njobs) return;
-        const BatchJob jb = jobs[j];
-        const unsigned long long t0 = globaltimer_ns();
-        TravParams p = job_params(jb, scratch, hub_degree, &s_ctl);
+        if (threadIdx.x == 0) {
+            const BatchJob jb = jobs[j];
+            s_p = job_params(jb, scratch, hub_degree, &s_ctl);
+            s_app = jb.app;
+            s_t0 = globaltimer_ns();
+        }
+        __syncthreads();
+        const unsigned long long t0 = s_t0;
         CtaMode m{&s_ctl, threadIdx.x, BLOCK, w, BLOCK / 32, 0};
-        if (jb.app == 1) sssp_body(p, m, s_near[w], s_far[w]);
-        else bfs_body(p, m, s_near[w]);
+        if (s_app == 1) sssp_body(s_p, m, s_near[w], s_far[w]);
+        else bfs_body(s_p, m, s_near[w]);
         __syncthreads();
         if (threadIdx.x == 0) write_result(jobs[j], s_ctl, t0);
         __syncthreads();
@@ -240,6 +256,7 @@ void fill_batch_job(BatchJob &j, const gft_query &x, uint32_t hub_degree)
     j.hub_cap = (uint32_t)std::min<uint64_t>(G.nnodes, (uint64_t)G.nedges / hub_degree + 1);
     j.vec_ok = ((uintptr_t)G.edge_dst % 16 == 0) && (!G.edge_data || (uintptr_t)G.edge_data % 16 == 0);
     j.uniform = G.max_degree <= kUniformDegree;
+    j.dir_opt = x.app == 0 && G.symmetric;
 }
 
 // Bytes of scratch one CTA-mode job needs (layout of batch_kernel).

@@ -70,7 +70,8 @@ struct gft_server {
     std::vector<Lane> lanes;
     std::mutex mu;
     std::condition_variable cv_work, cv_done;
-    std::deque<uint64_t> pending;
+    std::deque<uint64_t> pending;       // requests for the shared lanes
+    std::deque<uint64_t> wide_pending;  // requests for the wide pool
     std::unordered_map<uint64_t, Req> reqs;
     std::deque<gft_completion> done;
     uint64_t next_ticket = 1;
@@ -95,6 +96,16 @@ static bool runs_on_group(const gft_server *s, const gft_query &q)
     if (s->cfg.group_blocks <= 1 || G.nnodes < s->cfg.group_min_nodes) return false;
     const bool sparse = (uint64_t)G.nedges < (uint64_t)s->cfg.sparse_degree * G.nnodes;
     return !(q.app == 0 && sparse);
+}
+
+// SSSP on a large skewed-degree graph (R-MAT-like): such a query moves so
+// much memory that it runs no faster side by side than alone, and it takes
+// many times longer on a narrow group.  It runs on the wide pool: lanes
+// [0, wide_lanes), one request at a time.
+static bool is_wide(const gft_server *s, const gft_query &q)
+{
+    const DeviceGraph &G = q.graph->g;
+    return s->cfg.wide_lanes > 0 && q.app == 1 && G.max_degree > kUniformDegree && G.nedges >= s->cfg.wide_min_edges;
 }
 
 static void complete(gft_server *s, uint64_t t, gft_status st, uint32_t levels, uint64_t edges, double t_done)
@@ -174,7 +185,7 @@ static void dispatcher_loop(gft_server *s)
     while (true) {
         bool idle = true;
         std::unique_lock<std::mutex> lk(s->mu);
-        if (s->stop && s->pending.empty()) {
+        if (s->stop && s->pending.empty() && s->wide_pending.empty()) {
             bool any_busy = false;
             for (auto &l : s->lanes) any_busy |= l.busy;
             if (!any_busy) break;
@@ -203,8 +214,26 @@ static void dispatcher_loop(gft_server *s)
         if (!s->done.empty()) s->cv_done.notify_all();
         // Dispatch, in arrival order: a heavy request runs alone on a fair
         // share of the free lanes; a run of light requests shares one lane.
+        // The wide pool takes the oldest wide request once all its lanes are
+        // free, plus every free shared lane when no other request waits.
+        const uint32_t W = s->cfg.wide_lanes;
+        if (!s->wide_pending.empty()) {
+            bool pool_free = true;
+            for (uint32_t li = 0; li < W; li++) pool_free &= !s->lanes[li].busy;
+            if (pool_free) {
+                std::vector<uint64_t> big{s->wide_pending.front()}, none;
+                s->wide_pending.pop_front();
+                std::vector<uint32_t> lent;
+                for (uint32_t li = 1; li < W; li++) lent.push_back(li);
+                if (s->pending.empty())
+                    for (uint32_t li = W; li < s->lanes.size(); li++)
+                        if (!s->lanes[li].busy) lent.push_back(li);
+                launch_lane(s, 0, big, none, lent);
+                idle = false;
+            }
+        }
         std::vector<uint32_t> free_lanes;
-        for (uint32_t li = 0; li < s->lanes.size(); li++)
+        for (uint32_t li = W; li < s->lanes.size(); li++)
             if (!s->lanes[li].busy) free_lanes.push_back(li);
         size_t fi = 0;
         while (fi < free_lanes.size() && !s->pending.empty()) {
@@ -260,6 +289,8 @@ gft_status gft_serve_config_default(gft_serve_config *cfg)
     cfg->sparse_degree = 0;
     cfg->queue_capacity = 1u << 20;
     cfg->max_lanes_per_request = 0;  // all lanes
+    cfg->wide_lanes = GFT_SERVE_AUTO;  // 4/9 of the lanes when there are at least 4
+    cfg->wide_min_edges = 1u << 25;
     return GFT_OK;
 }
 
@@ -290,6 +321,8 @@ gft_status gft_serve_open(gft_engine *e, const gft_serve_config *cfg_in, gft_ser
         s->cfg.lanes = std::max(1u, (uint32_t)resident / s->cfg.lane_blocks);
     if (s->cfg.max_lanes_per_request == 0 || s->cfg.max_lanes_per_request > s->cfg.lanes)
         s->cfg.max_lanes_per_request = s->cfg.lanes;
+    if (s->cfg.wide_lanes == GFT_SERVE_AUTO) s->cfg.wide_lanes = s->cfg.lanes >= 4 ? (s->cfg.lanes * 4 + 8) / 9 : 0;
+    if (s->cfg.wide_lanes >= s->cfg.lanes) s->cfg.wide_lanes = s->cfg.lanes - 1;
     cudaError_t err = cudaSetDevice(e->device);
     s->lanes.resize(s->cfg.lanes);
     for (auto &l : s->lanes) {
@@ -330,7 +363,7 @@ gft_status gft_serve_enqueue(gft_server *s, const gft_query *q, uint64_t *ticket
     r.t_arrive = now_ms();
     s->reqs.emplace(t, r);
     s->in_flight++;
-    s->pending.push_back(t);
+    (is_wide(s, *q) ? s->wide_pending : s->pending).push_back(t);
     s->cv_work.notify_one();
     *ticket = t;
     return GFT_OK;

@@ -308,7 +308,10 @@ GFT_API void gft_batch_destroy(gft_batch *b);
  * lower average degree counts as light) runs alone as one CTA group over
  * w free lanes, w = free lanes / heavy requests waiting, at least 1 and at
  * most `max_lanes_per_request`: on an idle server a request gets the whole
- * device, under load requests share it lane by lane.  A run of light
+ * device, under load requests share it lane by lane.  SSSP on a large
+ * skewed graph (see wide_lanes) instead runs on a reserved pool of lanes,
+ * one request at a time, taking every free lane when nothing else waits:
+ * such a query moves so much memory that it gains nothing side by side.  A run of light
  * requests shares one launch on one lane, one CTA each.  A request that
  * arrives while others run starts as soon as a lane and arena space are
  * free, and a long request never holds up a launch of short ones.  A
@@ -329,7 +332,15 @@ typedef struct gft_serve_config {
     uint32_t sparse_degree;     /* default 0 (no exception)                      */
     uint32_t queue_capacity;    /* requests admitted but not completed           */
     uint32_t max_lanes_per_request; /* widest heavy launch (0 = all lanes)       */
+    uint32_t wide_lanes;        /* lanes reserved for wide requests: SSSP on a
+                                   graph with a vertex of degree > 32 and at
+                                   least wide_min_edges edges.  They run one at
+                                   a time on the whole pool (GFT_SERVE_AUTO =
+                                   4/9 of the lanes when there are >= 4; 0 =
+                                   no pool)                                   */
+    uint32_t wide_min_edges;    /* default 2^25                                */
 } gft_serve_config;
+#define GFT_SERVE_AUTO 0xFFFFFFFFu
 
 typedef struct gft_completion {
     uint64_t ticket;

@@ -93,3 +93,37 @@ def test_poisson_load_smoke(gft, engine):
     srv.close()
     assert r["failures"] == 0 and r["requests"] == 400
     assert r["p99_ms"] is not None and r["p99_ms"] >= r["p50_ms"] > 0
+
+
+def test_wide_pool_for_skewed_sssp(gft, engine):
+    """SSSP on a skewed graph of at least wide_min_edges edges runs on the
+    reserved wide pool (lane 1 onwards, many lanes at once), everything else
+    on the shared lanes; every result equals the query run alone."""
+    import torch
+
+    from galoisgpu_b200.serve import Server
+
+    rm = gft.CSRGraph.rmat(13, 8, seed=41, max_weight=255)
+    rd = gft.CSRGraph.road(90, seed=42)
+    devs = [rm.copy_to_gpu(), rd.copy_to_gpu()]
+    srv = Server(engine, group_min_nodes=1 << 10, group_blocks=8, lane_arena_bytes=64 << 20, wide_min_edges=1)
+    reqs = []
+    for i in range(48):
+        gi, app = i % 2, ("sssp" if i % 3 else "bfs")
+        host = (rm, rd)[gi]
+        src = host.pick_sources(500 + i, 1)[0]
+        out = torch.full((devs[gi].nnodes,), -5, dtype=torch.int32, device="cuda")
+        reqs.append((srv.enqueue(devs[gi], app, src, out, delta=300), gi, app, src, out))
+    got = {}
+    while len(got) < len(reqs):
+        for c in srv.poll(256, 100000):
+            got[c["ticket"]] = c
+    srv.close()
+    wide = [got[t] for t, gi, app, _, _ in reqs if gi == 0 and app == "sssp"]
+    assert wide and all(c["lane"] == 1 and c["width"] >= 2 for c in wide)
+    others = [got[t] for t, gi, app, _, _ in reqs if not (gi == 0 and app == "sssp")]
+    assert all(c["lane"] > 1 for c in others), "shared requests never start on the wide pool"
+    for t, gi, app, src, out in reqs:
+        assert got[t]["status"] == 0
+        alone = (engine.sssp(devs[gi], src, delta=300) if app == "sssp" else engine.bfs(devs[gi], src))["out"]
+        np.testing.assert_array_equal(out.cpu().numpy(), alone.cpu().numpy())
