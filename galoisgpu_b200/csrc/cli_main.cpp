@@ -2,10 +2,14 @@
 //
 //   bfs  [-q] [-g gpunum] [-o output-file] [-l] [-s startNode] graph-file
 //   sssp [-q] [-g gpunum] [-o output-file] [-l] [-d delta] [-s startNode] graph-file
+//   cc   [-q] [-g gpunum] [-o output-file] graph-file
 //
 // Same options, same stdout/stderr lines and same output file as the
-// reference driver (skelapp/skel.cu:37-151 with apps/bfs/support.cu:5-45 and
-// apps/sssp/support.cu:6-53).  The traversal runs through the C ABI.  `-l`
+// reference driver (skelapp/skel.cu:37-151 with apps/bfs/support.cu:5-45,
+// apps/sssp/support.cu:6-53 and apps/cc/support.cu:3-36; cc prints the
+// reference's "components: N" line, apps/cc/kernel.cu:719).  CC labels are
+// the smallest vertex id of each component, where the reference's are
+// whichever roots its racy hooks leave: the partition is the same.  The traversal runs through the C ABI.  `-l`
 // (the reference's host-driven load balancer, apps/bfs/kernel.cu:286-311) is
 // accepted for compatibility; this engine always balances per vertex inside
 // its persistent kernel.  Errors are reported and turned into a non-zero
@@ -21,13 +25,16 @@
 
 #include "gft.h"
 
-#ifndef GFT_CLI_SSSP
-#define GFT_CLI_SSSP 0
+// The app this binary is: 0 bfs, 1 sssp, 2 cc (set by the build).
+#ifndef GFT_CLI_APP
+#define GFT_CLI_APP 0
 #endif
+#define GFT_CLI_SSSP (GFT_CLI_APP == 1)
+#define GFT_CLI_CC (GFT_CLI_APP == 2)
 
-static const char *kAppOpts = GFT_CLI_SSSP ? "ls:d:" : "ls:";
-static const char *kAppUsage = GFT_CLI_SSSP ? "[-l] [-d delta] [-s startNode]" : "[-l] [-s startNode]";
-static const char *kAppArgsUsage = "-l: enable thread block load balancer (by default false)";
+static const char *kAppOpts = GFT_CLI_CC ? "" : GFT_CLI_SSSP ? "ls:d:" : "ls:";
+static const char *kAppUsage = GFT_CLI_CC ? "" : GFT_CLI_SSSP ? "[-l] [-d delta] [-s startNode]" : "[-l] [-s startNode]";
+static const char *kAppArgsUsage = GFT_CLI_CC ? "" : "-l: enable thread block load balancer (by default false)";
 
 static void usage(const char *argv0)
 {
@@ -96,15 +103,15 @@ int main(int argc, char **argv)
     }
     const char *input = argv[optind];
 
-    fprintf(stderr, "OPTIONS: gft engine (libgft %d, sm_100a persistent %s)\n", gft_version(),
-            GFT_CLI_SSSP ? "near-far SSSP" : "BFS");
+    fprintf(stderr, "OPTIONS: gft engine (libgft %d, sm_100a %s)\n", gft_version(),
+            GFT_CLI_CC ? "union-find CC" : GFT_CLI_SSSP ? "persistent near-far SSSP" : "persistent BFS");
     gft_csr h;
     uint64_t t0 = now_ns();
     gft_status s = gft_gr_read(input, &h);
     if (s != GFT_OK) return die("read", s);
     printf("nnodes=%u, nedges=%u.\n", h.nnodes, h.nedges);
     printf("read %s in %llu ms\n", input, (unsigned long long)((now_ns() - t0) / 1000000));
-    if ((uint32_t)start_node >= h.nnodes) {
+    if (!GFT_CLI_CC && (uint32_t)start_node >= h.nnodes) {
         fprintf(stderr, "start node %d out of range (%u nodes)\n", start_node, h.nnodes);
         gft_csr_free(&h);
         return EXIT_FAILURE;
@@ -118,16 +125,20 @@ int main(int argc, char **argv)
     std::vector<int32_t> val(h.nnodes);
     gft_stats st;
     memset(&st, 0, sizeof st);
+    uint64_t comps = 0;
     uint64_t k0 = now_ns();
-    if (GFT_CLI_SSSP) {
+    if (GFT_CLI_CC) {
+        s = gft_cc_host(e, g, val.data(), nullptr, nullptr, &st, &comps);
+    } else if (GFT_CLI_SSSP) {
         printf("delta: %d\n", delta);
         s = gft_sssp_host(e, g, (uint32_t)start_node, delta, val.data(), nullptr, nullptr, nullptr, &st);
     } else {
         s = gft_bfs_host(e, g, (uint32_t)start_node, val.data(), nullptr, nullptr, nullptr, &st);
     }
     uint64_t k1 = now_ns();
-    if (s != GFT_OK) return die(GFT_CLI_SSSP ? "sssp" : "bfs", s);
+    if (s != GFT_OK) return die(GFT_CLI_CC ? "cc" : GFT_CLI_SSSP ? "sssp" : "bfs", s);
     if (GFT_CLI_SSSP) printf("iterations: %u\n", st.levels);
+    if (GFT_CLI_CC) printf("components: %llu\n", (unsigned long long)comps);
     printf("gg_main %llu %llu\n", (unsigned long long)k0, (unsigned long long)k1);
     fprintf(stderr, "Total time: %llu ms\n", (unsigned long long)((k1 - k0) / 1000000));
     fprintf(stderr, "Total time: %llu ns\n", (unsigned long long)(k1 - k0));
@@ -135,7 +146,8 @@ int main(int argc, char **argv)
             st.iterations);
     int rc = 0;
     if (!quiet && output) {
-        if ((s = gft_write_output(output, h.nnodes, val.data())) != GFT_OK) rc = die("output", s);
+        s = GFT_CLI_CC ? gft_write_cc_output(output, &h, val.data()) : gft_write_output(output, h.nnodes, val.data());
+        if (s != GFT_OK) rc = die("output", s);
     }
     gft_engine_destroy(e);
     gft_graph_free(g);

@@ -278,4 +278,47 @@ gft_status gft_write_output(const char *path, uint32_t nnodes, const int32_t *h_
     return GFT_OK;
 }
 
+gft_status gft_write_cc_output(const char *path, const gft_csr *g, const int32_t *h_label)
+{
+    if (!path || !g || !g->row_start || (g->nnodes && !h_label) || (g->nedges && !g->edge_dst))
+        return fail(GFT_ERR_INVALID_ARG, "gft_write_cc_output: null argument");
+    bool to_stdout = strcmp(path, "-") == 0;
+    FILE *f = to_stdout ? stdout : fopen(path, "w");
+    if (!f) return fail(GFT_ERR_IO, "gft_write_cc_output: cannot open %s: %s", path, strerror(errno));
+    // apps/cc/support.cu:16-36: per node "%d %d\n" (id, label), then per
+    // out-edge j "\te %d: %d %d %d\n" (j, dst, edge_data[j], label[dst]);
+    // edge_data is 0 for an unweighted graph.  Formatted in parallel blocks of
+    // nodes, written in order.
+    const uint32_t n = g->nnodes, block = 1u << 18;
+    uint32_t nblocks = (n + block - 1) / block;
+    bool ok = true;
+    unsigned nt = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+    for (uint32_t b0 = 0; b0 < nblocks && ok; b0 += nt) {
+        uint32_t nb = std::min<uint32_t>(nt, nblocks - b0);
+        std::vector<std::string> text(nb);
+        std::vector<std::thread> th;
+        for (uint32_t t = 0; t < nb; t++)
+            th.emplace_back([&, t] {
+                uint32_t lo = (b0 + t) * block, hi = std::min<uint32_t>(n, lo + block);
+                std::string &s = text[t];
+                s.reserve((size_t)(hi - lo) * 16 + (size_t)(g->row_start[hi] - g->row_start[lo]) * 32);
+                char line[96];
+                for (uint32_t i = lo; i < hi; i++) {
+                    s.append(line, snprintf(line, sizeof line, "%d %d\n", (int)i, h_label[i]));
+                    for (uint32_t j = g->row_start[i]; j < g->row_start[i + 1]; j++) {
+                        const uint32_t d = g->edge_dst[j];
+                        s.append(line, snprintf(line, sizeof line, "\te %d: %d %d %d\n", (int)j, (int)d,
+                                                g->edge_data ? g->edge_data[j] : 0, h_label[d]));
+                    }
+                }
+            });
+        for (auto &x : th) x.join();
+        for (auto &s : text) ok = ok && write_all(f, s.data(), s.size());
+    }
+    if (to_stdout) fflush(f);
+    else if (fclose(f) != 0) ok = false;
+    if (!ok) return fail(GFT_ERR_IO, "gft_write_cc_output: write to %s failed", path);
+    return GFT_OK;
+}
+
 }  // extern "C"

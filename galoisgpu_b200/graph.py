@@ -374,6 +374,28 @@ class Engine:
         res["levels_of"] = levels
         return res
 
+    def cc(self, graph: DeviceGraph, out=None, tune: Tune | None = None, stream=None) -> dict:
+        """Connected components (apps/cc): ``out[v]`` (int32 device tensor)
+        becomes the smallest vertex id of v's weakly connected component.
+        Returns the stats plus ``components``."""
+        import torch
+
+        dev = torch.device("cuda", graph.device)
+        if out is None:
+            out = torch.empty(graph.nnodes, dtype=torch.int32, device=dev)
+        st, comps = Stats(), C.c_uint64()
+        check(load().gft_cc(self._h, graph.handle, C.c_void_p(out.data_ptr()), self._tune(tune),
+                            _stream_ptr(stream if stream is not None else torch.cuda.current_stream(dev)),
+                            C.byref(st), C.byref(comps)))
+        return {"out": out, "components": comps.value, **st.as_dict()}
+
+    def cc_host(self, graph: DeviceGraph, out: np.ndarray, tune: Tune | None = None, stream=None) -> dict:
+        """Connected components into a host int32 array (end to end)."""
+        st, comps = Stats(), C.c_uint64()
+        check(load().gft_cc_host(self._h, graph.handle, C.c_void_p(out.ctypes.data), self._tune(tune),
+                                 _stream_ptr(stream), C.byref(st), C.byref(comps)))
+        return {"components": comps.value, **st.as_dict()}
+
     def bfs_host(self, graph: DeviceGraph, start_node: int, out: np.ndarray, parent: np.ndarray | None = None,
                  tune: Tune | None = None, stream=None) -> dict:
         """End-to-end query with host result buffers (int32 / uint32 numpy)."""
@@ -482,6 +504,14 @@ def output(path: str | Path, values: np.ndarray) -> None:
     check(load().gft_write_output(str(path).encode(), len(v), C.c_void_p(v.ctypes.data)))
 
 
+def write_cc_output(path: str | Path, graph: CSRGraph, labels: np.ndarray) -> None:
+    """CC labels in the reference's format: a node line and one line per
+    out-edge (apps/cc/support.cu:16-36)."""
+    lab = np.ascontiguousarray(labels, dtype=np.int32)
+    c = graph._csr()
+    check(load().gft_write_cc_output(str(path).encode(), C.byref(c), C.c_void_p(lab.ctypes.data)))
+
+
 __all__ = [
     "Batch",
     "CSRGraph",
@@ -493,5 +523,6 @@ __all__ = [
     "DEFAULT_DELTA",
     "reach_stats",
     "output",
+    "write_cc_output",
     "_lib",
 ]

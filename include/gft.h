@@ -388,6 +388,27 @@ GFT_API gft_status gft_msbfs(gft_engine *e, const gft_graph *g, const uint32_t *
 GFT_API gft_status gft_msbfs_levels(const uint32_t *d_planes, uint32_t nnodes, uint32_t k, uint32_t levels, uint32_t i,
                                     int32_t *d_out, void *stream);
 
+/* ---------------------------------------------------------------------------
+ * Connected components: replaces apps/cc gg_main (apps/cc/kernel.cu:630-723),
+ * whose result is node_data.  d_label[v] (int32, nnodes entries) becomes the
+ * smallest vertex id of v's weakly connected component: every edge joins its
+ * endpoints, as the reference's hooks treat it (:249-330).  The reference's
+ * own labels are whichever roots its racy hooks leave, so only its
+ * partition and its count ("components: N", :449-462,719) are comparable;
+ * these labels do not depend on the schedule.  *components receives the
+ * number of components.  On a graph marked symmetric each undirected edge is
+ * joined once.
+ * ------------------------------------------------------------------------- */
+GFT_API gft_status gft_cc(gft_engine *e, const gft_graph *g, int32_t *d_label, const gft_tuning *tune, void *stream,
+                          gft_stats *stats, uint64_t *components);
+GFT_API gft_status gft_cc_host(gft_engine *e, const gft_graph *g, int32_t *h_label, const gft_tuning *tune,
+                               void *stream, gft_stats *stats, uint64_t *components);
+/* Writes CC labels in the reference's output format (apps/cc/support.cu:
+ * 16-36): per node "%d %d\n", then one "\te %d: %d %d %d\n" line per out-edge
+ * (edge index, destination, edge_data or 0, destination's label).  The host
+ * CSR supplies the edges.  path "-" writes to stdout. */
+GFT_API gft_status gft_write_cc_output(const char *path, const gft_csr *g, const int32_t *h_label);
+
 /* Reach statistics of a result already on the device: V_r (vertices with a
  * finite value) and E_r (sum of their out-degrees, the edges a top-down
  * traversal must scan).  Waits for `stream`. */

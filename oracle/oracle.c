@@ -18,11 +18,23 @@
  *                                 atomicMin), :455-478 (driver)
  *   - output text                 apps/bfs/support.cu:27-45,
  *                                 apps/sssp/support.cu:34-53
+ *   - connected components        apps/cc/kernel.cu:18-29 (init: label v),
+ *                                 :249-330 (hooking over every edge, both
+ *                                 endpoints), :449-462 (a component is a
+ *                                 vertex that is its own label),
+ *                                 apps/cc/support.cu:16-36 (output)
  *
  * The reference's BFS and SSSP results are schedule independent: BFS levels
  * are hop distances and SSSP distances are the unique shortest-path lengths
  * (atomicMin is monotone), so a FIFO BFS and a binary-heap Dijkstra give the
  * same numbers bit for bit as long as no distance overflows int32.
+ *
+ * The reference's CC labels are not canonical: its hooks are racy plain
+ * stores (apps/cc/kernel.cu:263,293,329), so which vertex of a component
+ * ends up as the label depends on the schedule.  The partition into
+ * components is not, and neither is the count.  This restatement labels
+ * every vertex with the smallest vertex id of its component; parity with the
+ * reference is checked on the partition.
  *
  * Parity of this restatement is pinned against outputs of the reference's
  * own CUDA build (oracle/ref/Makefile builds it from the reference sources;
@@ -262,4 +274,58 @@ int64_t orc_read_output(const char *path, uint32_t nnodes, int32_t *val)
     }
     fclose(f);
     return n;
+}
+
+/* ------------------------------------------------------------------ */
+/* Connected components (weak: every edge joins its endpoints, as the   */
+/* reference's hooking treats it, apps/cc/kernel.cu:249-330).  label[v] */
+/* = the smallest vertex id of v's component.  Union-find with path     */
+/* halving; the smaller root always becomes the parent.  Returns the    */
+/* number of components (apps/cc/kernel.cu:449-462).                    */
+/* ------------------------------------------------------------------ */
+static uint32_t uf_find(uint32_t *p, uint32_t x)
+{
+    while (p[x] != x) {
+        p[x] = p[p[x]];
+        x = p[x];
+    }
+    return x;
+}
+
+uint64_t orc_cc(uint32_t nnodes, const uint32_t *row_start, const uint32_t *edge_dst, int32_t *label)
+{
+    uint32_t *p = (uint32_t *)malloc((size_t)(nnodes ? nnodes : 1) * 4);
+    for (uint32_t v = 0; v < nnodes; v++) p[v] = v;
+    for (uint32_t u = 0; u < nnodes; u++)
+        for (uint32_t e = row_start[u]; e < row_start[u + 1]; e++) {
+            uint32_t a = uf_find(p, u), b = uf_find(p, edge_dst[e]);
+            if (a < b) p[b] = a;
+            else if (b < a) p[a] = b;
+        }
+    uint64_t comps = 0;
+    for (uint32_t v = 0; v < nnodes; v++) {
+        label[v] = (int32_t)uf_find(p, v);
+        comps += label[v] == (int32_t)v;
+    }
+    free(p);
+    return comps;
+}
+
+/* CC output text as the reference writes it (apps/cc/support.cu:16-36):  */
+/* per node "%d %d\n" (id, label), then per out-edge j of that node        */
+/* "\te %d: %d %d %d\n" (j, dst, edge_data[j], label[dst]); edge_data is   */
+/* 0 for an unweighted graph (the reference's calloc'd array).             */
+int orc_write_cc_output(const char *path, uint32_t nnodes, const uint32_t *row_start, const uint32_t *edge_dst,
+                        const int32_t *edge_data, const int32_t *label)
+{
+    FILE *f = fopen(path, "w");
+    if (!f) return -1;
+    for (int i = 0; i < (int)nnodes; i++) {
+        fprintf(f, "%d %d\n", i, label[i]);
+        for (int j = (int)row_start[i]; j < (int)row_start[i + 1]; j++) {
+            uint32_t d = edge_dst[j];
+            fprintf(f, "\te %d: %d %d %d\n", j, (int)d, edge_data ? edge_data[j] : 0, label[d]);
+        }
+    }
+    return fclose(f) ? -2 : 0;
 }

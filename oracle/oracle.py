@@ -51,6 +51,10 @@ def load():
         lib.orc_write_output.argtypes = [C.c_char_p, C.c_uint32, C.c_void_p]
         lib.orc_read_output.restype = C.c_int64
         lib.orc_read_output.argtypes = [C.c_char_p, C.c_uint32, C.c_void_p]
+        lib.orc_cc.restype = C.c_uint64
+        lib.orc_cc.argtypes = [C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p]
+        lib.orc_write_cc_output.restype = C.c_int
+        lib.orc_write_cc_output.argtypes = [C.c_char_p, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
         _lib = lib
     return _lib
 
@@ -136,3 +140,36 @@ def read_output(path, nnodes: int) -> np.ndarray:
     if r != nnodes:
         raise ValueError(f"oracle: {path}: parsed {r} lines, expected {nnodes}")
     return v
+
+
+def cc(row_start, edge_dst) -> tuple[np.ndarray, int]:
+    """Connected components: (label per vertex = smallest vertex id of its
+    component, number of components)."""
+    rs = np.ascontiguousarray(row_start, dtype=np.uint32)
+    dst = np.ascontiguousarray(edge_dst, dtype=np.uint32)
+    n = len(rs) - 1
+    label = np.empty(max(n, 1), dtype=np.int32)[:n]
+    comps = load().orc_cc(n, _p(rs), _p(dst), _p(label))
+    return label, int(comps)
+
+
+def write_cc_output(path, row_start, edge_dst, edge_data, label) -> None:
+    rs = np.ascontiguousarray(row_start, dtype=np.uint32)
+    dst = np.ascontiguousarray(edge_dst, dtype=np.uint32)
+    w = None if edge_data is None else np.ascontiguousarray(edge_data, dtype=np.int32)
+    lab = np.ascontiguousarray(label, dtype=np.int32)
+    rc = load().orc_write_cc_output(str(path).encode(), len(rs) - 1, _p(rs), _p(dst), _p(w) if w is not None else None,
+                                    _p(lab))
+    if rc != 0:
+        raise OSError(f"orc_write_cc_output({path}) failed: {rc}")
+
+
+def canonical_labels(label) -> np.ndarray:
+    """Relabels a partition so every vertex carries the smallest vertex id of
+    its class: the form in which partitions from different labelings (the
+    reference's schedule-dependent roots, this oracle's minima) compare."""
+    lab = np.asarray(label, dtype=np.int64)
+    n = len(lab)
+    first = np.full(max(n, int(lab.max()) + 1 if n else 0), n, dtype=np.int64)
+    np.minimum.at(first, lab, np.arange(n, dtype=np.int64))
+    return first[lab].astype(np.int32)

@@ -3,8 +3,9 @@
  * -Xlinker --wrap=cudaLaunchKernel,--wrap=cudaMalloc.  Test harness only.
  *
  * 1. Cooperative launch of the persistent drivers.
- * The reference's persistent drivers gg_main_pipe_1_gpu_gb
- * (apps/bfs/kernel.cu:375, apps/sssp/kernel.cu:448) synchronise their CTAs
+ * The reference's persistent drivers gg_main_pipe_N_gpu_gb
+ * (apps/bfs/kernel.cu:375, apps/sssp/kernel.cu:448, apps/cc/kernel.cu:481,569)
+ * synchronise their CTAs
  * with a software grid barrier that spins without a limit
  * (rt/include/gbar.cuh:84-120), sized by a hand-written occupancy table
  * (rt/include/cuda_launch_config.hpp:205-265).  A grid that is not fully
@@ -45,7 +46,7 @@ extern "C" cudaError_t __wrap_cudaLaunchKernel(const void *func, dim3 grid, dim3
         long long padded = (long long)*size * 4 + (4ll << 20);  // ints in the padded dwl allocation
         *size = (int)(padded > 0x7FFFFFFFll ? 0x7FFFFFFFll : padded);
     }
-    if (name && strstr(name, "gg_main_pipe_1_gpu_gb")) {
+    if (name && strstr(name, "_gpu_gb")) {  // gg_main_pipe_N_gpu_gb: bfs, sssp, cc
         cudaError_t e = cudaLaunchCooperativeKernel(func, grid, block, args, smem, stream);
         if (e != cudaSuccess)
             fprintf(stderr, "oracle-ref: cooperative launch of %s (%u x %u) refused: %s\n", name, grid.x,

@@ -91,17 +91,18 @@ def test_last_error_is_per_thread(gft):
 
 
 def test_cli_binaries_are_the_right_apps():
-    """bin/bfs takes the BFS options of apps/bfs/support.cu (no -d) and
-    bin/sssp adds -d (apps/sssp/support.cu); both print the usage and exit
-    non-zero without arguments, which needs no GPU."""
+    """bin/bfs takes the BFS options of apps/bfs/support.cu (no -d),
+    bin/sssp adds -d (apps/sssp/support.cu) and bin/cc takes neither -s nor
+    -d (apps/cc/support.cu); each prints the usage and exits non-zero
+    without arguments, which needs no GPU."""
     import subprocess
 
     from galoisgpu_b200 import build as b
 
     if not (b.BIN / "bfs").exists():
         b.build()
-    for app, has_delta in (("bfs", False), ("sssp", True)):
+    for app, has_delta, has_src in (("bfs", False, True), ("sssp", True, True), ("cc", False, False)):
         r = subprocess.run([str(b.BIN / app)], capture_output=True, text=True, timeout=60)
         assert r.returncode != 0
-        assert "usage:" in r.stderr and "[-s startNode]" in r.stderr
+        assert "usage:" in r.stderr and ("[-s startNode]" in r.stderr) == has_src, r.stderr
         assert ("-d delta" in r.stderr) == has_delta, r.stderr
