@@ -17,11 +17,16 @@
 // vertex id of its (weakly) connected component.  Unlike the reference's
 // labels, these do not depend on the schedule.
 //
-// Launches, on the caller's stream: init; hook over 32-vertex blocks with the
-// lanes' edge lists flattened across the warp (vertices of degree >=
-// kCcHubDegree go to a hub list instead); hook of the hub edges in
-// kCcHubChunk-edge chunks; compress + count.  On a graph marked symmetric
-// each undirected edge is joined once, from its larger endpoint.
+// Launches, on the caller's stream.  On a graph marked symmetric, the sampled
+// pass of Afforest (Sutton, Ben-Nun, Barak, IPDPS 2018): init; two rounds of
+// each vertex joining its next neighbour, each followed by a flatten; one
+// CTA samples 1024 labels for
+// the giant component; hook of the remaining edges of every vertex outside
+// it; hook of those vertices' hub edges; compress + count.  Otherwise every
+// edge is hooked: init; hook; hub hook; compress + count.  The hook flattens
+// the edge lists of 32 vertices across the warp; vertices of degree >=
+// kCcHubDegree go to a hub list, whose edges are hooked in kCcHubChunk-edge
+// chunks.
 #include <string.h>
 
 #include <algorithm>
@@ -78,25 +83,34 @@ __global__ void cc_init(uint32_t *label, uint32_t n, unsigned long long *counter
 
 // counters[0] = (hubs << 32) | hub chunks, counters[1] = edges joined,
 // counters[2] = components.
+// mode 0: every edge, each undirected edge once on a graph marked symmetric
+//         (half_edges).  mode 1 (sampled, symmetric graphs only): the edges
+//         from index `first` on of every vertex outside the sampled giant
+//         component (its compressed label differs from *giant), in both
+//         directions, since the other endpoint may be skipped.
 __global__ void cc_hook(const uint32_t *__restrict__ row_start, const uint32_t *__restrict__ edge_dst, uint32_t n,
-                        uint32_t *label, uint2 *hubs, uint32_t hub_cap, int symmetric, unsigned long long *counters,
-                        unsigned *error)
+                        uint32_t *label, uint2 *hubs, uint32_t hub_cap, int half_edges, uint32_t first,
+                        const uint32_t *giant, unsigned long long *counters, unsigned *error)
 {
     const unsigned lane = threadIdx.x & 31;
     const uint32_t gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nwarps = (gridDim.x * blockDim.x) >> 5;
+    const uint32_t skip = giant ? __ldcg(giant) : 0xFFFFFFFFu;
     unsigned long long joined = 0;
     for (uint32_t base = gwarp * 32; base < n; base += nwarps * 32) {  // warp-uniform trip count
         const uint32_t u = base + lane;
         uint32_t start = 0, deg = 0;
-        if (u < n) {
+        if (u < n && (!giant || __ldcg(label + u) != skip)) {
             start = __ldg(row_start + u);
             deg = __ldg(row_start + u + 1) - start;
+            const uint32_t d0 = min(deg, first);
+            start += d0;
+            deg -= d0;
         }
         if (deg >= kCcHubDegree) {
             const unsigned nch = (deg + kCcHubChunk - 1) / kCcHubChunk;
             const unsigned long long old = atomicAdd(counters, (1ull << 32) | nch);
             const unsigned h = (unsigned)(old >> 32);
-            if (h < hub_cap) hubs[h] = make_uint2(u, (unsigned)old);
+            if (h < hub_cap) hubs[h] = make_uint2(u, (unsigned)old);  // its edges from `first` on
             else atomicExch(error, (unsigned)GFT_ERR_OVERFLOW);
             deg = 0;
         }
@@ -113,7 +127,7 @@ __global__ void cc_hook(const uint32_t *__restrict__ row_start, const uint32_t *
             const uint32_t ostart = __shfl_sync(kFull, start, j), oexcl = __shfl_sync(kFull, excl, j);
             if (g < total) {
                 const uint32_t src = base + j, dst = __ldcs(edge_dst + ostart + (g - oexcl));
-                if (!symmetric || dst < src) {
+                if (!half_edges || dst < src) {
                     cc_union(label, src, dst);
                     joined++;
                 }
@@ -125,7 +139,7 @@ __global__ void cc_hook(const uint32_t *__restrict__ row_start, const uint32_t *
 
 // Hub edges: chunk c belongs to hub h with hubs[h].y <= c < hubs[h+1].y.
 __global__ void cc_hook_hubs(const uint32_t *__restrict__ row_start, const uint32_t *__restrict__ edge_dst,
-                             uint32_t *label, const uint2 *hubs, uint32_t hub_cap, int symmetric,
+                             uint32_t *label, const uint2 *hubs, uint32_t hub_cap, int half_edges, uint32_t first,
                              unsigned long long *counters)
 {
     const unsigned lane = threadIdx.x & 31;
@@ -140,17 +154,72 @@ __global__ void cc_hook_hubs(const uint32_t *__restrict__ row_start, const uint3
             if (hubs[mid].y <= c) lo = mid;
             else hi = mid;
         }
-        const uint32_t u = hubs[lo].x, start = __ldg(row_start + u), deg = __ldg(row_start + u + 1) - start;
+        const uint32_t u = hubs[lo].x, start = __ldg(row_start + u) + first,
+                       deg = __ldg(row_start + u + 1) - start;
         const uint32_t off = (c - hubs[lo].y) * kCcHubChunk, len = min(kCcHubChunk, deg - off);
         for (uint32_t i = lane; i < len; i += 32) {
             const uint32_t dst = __ldcs(edge_dst + start + off + i);
-            if (!symmetric || dst < u) {
+            if (!half_edges || dst < u) {
                 cc_union(label, u, dst);
                 joined++;
             }
         }
     }
     warp_add_u64(counters + 1, joined, lane);
+}
+
+// Sampled pass, step 1: each vertex joins its r-th neighbour (a thread per
+// vertex; bounded work whatever the degree), for r < kCcSampleEdges, with a
+// flatten after each round so that the next round's finds are short (on a
+// grid, the first neighbours alone chain whole columns).
+constexpr uint32_t kCcSampleEdges = 2;
+
+__global__ void cc_neighbour_round(const uint32_t *__restrict__ row_start, const uint32_t *__restrict__ edge_dst,
+                                   uint32_t n, uint32_t r, uint32_t *label, unsigned long long *counters)
+{
+    const unsigned lane = threadIdx.x & 31;
+    const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, nthreads = gridDim.x * blockDim.x;
+    unsigned long long joined = 0;
+    for (uint32_t v = tid; v < n; v += nthreads) {
+        const uint32_t s = __ldg(row_start + v);
+        if (s + r < __ldg(row_start + v + 1)) {
+            cc_union(label, v, __ldcs(edge_dst + s + r));
+            joined++;
+        }
+    }
+    warp_add_u64(counters + 1, joined, lane);
+}
+
+// Every label becomes its root (no union runs concurrently).
+__global__ void cc_flatten(uint32_t *label, uint32_t n)
+{
+    const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, nthreads = gridDim.x * blockDim.x;
+    for (uint32_t v = tid; v < n; v += nthreads) {
+        uint32_t r = v, p;
+        while ((p = __ldcg(label + r)) != r) r = p;
+        label[v] = r;
+    }
+}
+
+// Sampled pass, step 2: the most frequent label among kCcSamples vertices
+// drawn with a fixed multiplicative hash (one CTA).  A tie or a poor sample
+// only skips fewer edges later; correctness never depends on it.
+constexpr int kCcSamples = 1024;
+
+__global__ void __launch_bounds__(kCcSamples, 1) cc_sample_giant(const uint32_t *label, uint32_t n, uint32_t *giant)
+{
+    __shared__ uint32_t s_lab[kCcSamples];
+    __shared__ unsigned long long s_best;
+    const uint32_t i = threadIdx.x;
+    const uint32_t v = (uint32_t)(((unsigned long long)(i * 2654435761u + 12345u) * n) >> 32);
+    s_lab[i] = n ? __ldcg(label + v) : 0;
+    if (i == 0) s_best = 0;
+    __syncthreads();
+    uint32_t count = 0;
+    for (int j = 0; j < kCcSamples; j++) count += s_lab[j] == s_lab[i];
+    atomicMax(&s_best, ((unsigned long long)count << 32) | (0xFFFFFFFFu - s_lab[i]));
+    __syncthreads();
+    if (i == 0) *giant = 0xFFFFFFFFu - (uint32_t)s_best;
 }
 
 // Final labels.  No union runs any more, so the walk to the root only
@@ -185,11 +254,12 @@ gft_status run_cc(gft_engine *e, const gft_graph *g, int32_t *d_label, const gft
     GFT_CUDA_TRY(cudaSetDevice(e->device));
     const uint32_t n = G.nnodes;
     const uint32_t hub_cap = std::max<uint32_t>(1, std::min<uint64_t>(n, (uint64_t)G.nedges / dev::kCcHubDegree + 1));
-    const size_t o_ctr = 0, o_err = 256, o_hubs = 512;
+    const size_t o_ctr = 0, o_err = 256, o_giant = 320, o_hubs = 512;
     GFT_TRY(e->scratch.ensure(o_hubs + (size_t)hub_cap * sizeof(uint2)));
     char *base = static_cast<char *>(e->scratch.ptr);
     unsigned long long *ctr = reinterpret_cast<unsigned long long *>(base + o_ctr);
     unsigned *err = reinterpret_cast<unsigned *>(base + o_err);
+    uint32_t *giant = reinterpret_cast<uint32_t *>(base + o_giant);
     uint2 *hubs = reinterpret_cast<uint2 *>(base + o_hubs);
     uint32_t *label = reinterpret_cast<uint32_t *>(d_label);
     const int block = 256;
@@ -199,11 +269,33 @@ gft_status run_cc(gft_engine *e, const gft_graph *g, int32_t *d_label, const gft
     GFT_CUDA_TRY(cudaEventRecord(e->ev0, stream));
     dev::cc_init<<<blocks, block, 0, stream>>>(label, n, ctr);
     GFT_CUDA_TRY(cudaGetLastError());
-    dev::cc_hook<<<blocks, block, 0, stream>>>(G.row_start, G.edge_dst, n, label, hubs, hub_cap, G.symmetric ? 1 : 0,
-                                               ctr, err);
-    GFT_CUDA_TRY(cudaGetLastError());
-    dev::cc_hook_hubs<<<blocks, block, 0, stream>>>(G.row_start, G.edge_dst, label, hubs, hub_cap,
-                                                    G.symmetric ? 1 : 0, ctr);
+    if (G.symmetric) {
+        // Sampled pass (Sutton, Ben-Nun, Barak, "Optimizing Parallel Graph
+        // Connectivity Computation via Subgraph Sampling", IPDPS 2018): join
+        // each vertex with its first neighbours, find the giant component
+        // from a sample, then join the remaining edges of the vertices
+        // outside it only.  An edge (v, w) skipped at v, which lies in the
+        // giant component, is joined at w unless w lies there too: on a
+        // symmetric graph every edge is also w's edge.
+        for (uint32_t r = 0; r < dev::kCcSampleEdges; r++) {
+            dev::cc_neighbour_round<<<blocks, block, 0, stream>>>(G.row_start, G.edge_dst, n, r, label, ctr);
+            GFT_CUDA_TRY(cudaGetLastError());
+            dev::cc_flatten<<<blocks, block, 0, stream>>>(label, n);
+            GFT_CUDA_TRY(cudaGetLastError());
+        }
+        dev::cc_sample_giant<<<1, dev::kCcSamples, 0, stream>>>(label, n, giant);
+        GFT_CUDA_TRY(cudaGetLastError());
+        dev::cc_hook<<<blocks, block, 0, stream>>>(G.row_start, G.edge_dst, n, label, hubs, hub_cap, 0,
+                                                   dev::kCcSampleEdges, giant, ctr, err);
+        GFT_CUDA_TRY(cudaGetLastError());
+        dev::cc_hook_hubs<<<blocks, block, 0, stream>>>(G.row_start, G.edge_dst, label, hubs, hub_cap, 0,
+                                                        dev::kCcSampleEdges, ctr);
+    } else {
+        dev::cc_hook<<<blocks, block, 0, stream>>>(G.row_start, G.edge_dst, n, label, hubs, hub_cap, 0, 0, nullptr,
+                                                   ctr, err);
+        GFT_CUDA_TRY(cudaGetLastError());
+        dev::cc_hook_hubs<<<blocks, block, 0, stream>>>(G.row_start, G.edge_dst, label, hubs, hub_cap, 0, 0, ctr);
+    }
     GFT_CUDA_TRY(cudaGetLastError());
     dev::cc_compress<<<blocks, block, 0, stream>>>(label, n, ctr);
     GFT_CUDA_TRY(cudaGetLastError());
@@ -220,7 +312,7 @@ gft_status run_cc(gft_engine *e, const gft_graph *g, int32_t *d_label, const gft
         float ms = 0;
         cudaEventElapsedTime(&ms, e->ev0, e->ev1);
         stats->levels = 1;
-        stats->iterations = 4;  // kernel launches
+        stats->iterations = G.symmetric ? 5 + 2 * dev::kCcSampleEdges : 4;  // kernel launches
         stats->vertices_reached = n;
         stats->edges_scanned = h[1];
         stats->kernel_ms = ms;

@@ -1,11 +1,13 @@
 """Times the reference's own CUDA build (oracle/_ref, built by
 oracle/ref/Makefile from the reference sources) on the full-size seeded
 configurations, the way a user runs it: ``bfs|sssp -q -s <src> [-d delta]
-<graph.gr>``, one process per query, reading its ``Total time: N ns`` line
+<graph.gr>`` or ``cc -q <graph.gr>``, one process per query, reading its
+``Total time: N ns`` line
 (reference skelapp/skel.cu:159-166; that time includes the worklist
 allocations gg_main makes, apps/bfs/kernel.cu:389, apps/sssp/kernel.cu:475).
 Kernel-only time comes from running this same script under
-``ncu --metrics gpu__time_duration.sum -k regex:gg_main_pipe``.
+``ncu --metrics gpu__time_duration.sum -k regex:gg_main_pipe`` (for cc, every
+kernel of the process: its driver is a host loop of launches).
 
 Test/measurement infrastructure only: the input graphs are produced with this
 repository's generator, and E_r comes from this repository's engine (whose
@@ -42,6 +44,8 @@ CONFIGS = {
     "rmat24": dict(kind="rmat", kw=dict(scale=24, edge_factor=16), seed=1, app="bfs", src_seed=2),
     "road1024": dict(kind="road", kw=dict(side=1024), seed=1, app="sssp", src_seed=1, delta=10000),
     "rmat20": dict(kind="rmat", kw=dict(scale=20, edge_factor=16), seed=1, app="bfs", src_seed=2),
+    "cc-rmat24": dict(kind="rmat", kw=dict(scale=24, edge_factor=16), seed=1, app="cc", src_seed=None),
+    "cc-road4096": dict(kind="road", kw=dict(side=4096), seed=1, app="cc", src_seed=None),
 }
 
 
@@ -66,6 +70,27 @@ def main(argv=None) -> int:
     eng = gft.Engine(0)
     delta = a.delta or c.get("delta")
     results = []
+    if c["app"] == "cc":
+        # Component count only: the reference's CC output lists every edge
+        # (apps/cc/support.cu:30-35), about 15 GB of text for RMAT-24.
+        mine = eng.cc(dg)
+        t = time.time()
+        r = subprocess.run([str(REF / "cc"), "-q", str(gr)], capture_output=True, text=True, timeout=1800)
+        wall = time.time() - t
+        if r.returncode != 0:
+            print(r.stdout, r.stderr, file=sys.stderr)
+            return r.returncode
+        m = re.search(r"Total time: (\d+) ns", r.stderr)
+        ns = int(m.group(1)) if m else None
+        comps = int(re.search(r"components: (\d+)", r.stdout).group(1))
+        rec = {"config": a.config, "app": "cc", "total_time_ns": ns, "edges": dg.nedges,
+               "gteps_total_time": dg.nedges / ns if ns else None, "components": comps,
+               "components_gft": mine["components"], "gft_kernel_ms": mine["kernel_ms"],
+               "parity_vs_gft": "same count" if comps == mine["components"] else "MISMATCH",
+               "process_wall_s": wall}
+        print(json.dumps(rec), flush=True)
+        gr.unlink()
+        return 0 if comps == mine["components"] else 1
     for i, s in enumerate(srcs):
         mine = (eng.sssp(dg, s, delta=delta) if c["app"] == "sssp" else eng.bfs(dg, s))["out"]
         v_r, e_r = gft.reach_stats(dg, mine)
