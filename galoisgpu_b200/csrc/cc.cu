@@ -18,9 +18,8 @@
 // labels, these do not depend on the schedule.
 //
 // Launches, on the caller's stream.  On a graph marked symmetric, the sampled
-// pass of Afforest (Sutton, Ben-Nun, Barak, IPDPS 2018): init; two rounds of
-// each vertex joining its next neighbour, each followed by a flatten; one
-// CTA samples 1024 labels for
+// pass of Afforest (Sutton, Ben-Nun, Barak, IPDPS 2018): init; each vertex
+// joins its first two neighbours; flatten; one CTA samples 1024 labels for
 // the giant component; hook of the remaining edges of every vertex outside
 // it; hook of those vertices' hub edges; compress + count.  Otherwise every
 // edge is hooked: init; hook; hub hook; compress + count.  The hook flattens
@@ -168,25 +167,26 @@ __global__ void cc_hook_hubs(const uint32_t *__restrict__ row_start, const uint3
     warp_add_u64(counters + 1, joined, lane);
 }
 
-// Sampled pass, step 1: each vertex joins its r-th neighbour (a thread per
-// vertex; bounded work whatever the degree), for r < kCcSampleEdges, with a
-// flatten after each round so that the next round's finds are short (on a
-// grid, the first neighbours alone chain whole columns).
+// Sampled pass, step 1: each vertex joins its first kCcSampleEdges
+// neighbours (a thread per vertex; bounded work whatever the degree).  One
+// flatten follows both rounds: a flatten between them was measured slower
+// on both RMAT-24 and the 4096^2 road grid.
 constexpr uint32_t kCcSampleEdges = 2;
 
-__global__ void cc_neighbour_round(const uint32_t *__restrict__ row_start, const uint32_t *__restrict__ edge_dst,
-                                   uint32_t n, uint32_t r, uint32_t *label, unsigned long long *counters)
+__global__ void cc_neighbour_rounds(const uint32_t *__restrict__ row_start, const uint32_t *__restrict__ edge_dst,
+                                    uint32_t n, uint32_t *label, unsigned long long *counters)
 {
     const unsigned lane = threadIdx.x & 31;
     const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, nthreads = gridDim.x * blockDim.x;
     unsigned long long joined = 0;
-    for (uint32_t v = tid; v < n; v += nthreads) {
-        const uint32_t s = __ldg(row_start + v);
-        if (s + r < __ldg(row_start + v + 1)) {
-            cc_union(label, v, __ldcs(edge_dst + s + r));
-            joined++;
+    for (uint32_t r = 0; r < kCcSampleEdges; r++)
+        for (uint32_t v = tid; v < n; v += nthreads) {
+            const uint32_t s = __ldg(row_start + v);
+            if (s + r < __ldg(row_start + v + 1)) {
+                cc_union(label, v, __ldcs(edge_dst + s + r));
+                joined++;
+            }
         }
-    }
     warp_add_u64(counters + 1, joined, lane);
 }
 
@@ -277,12 +277,10 @@ gft_status run_cc(gft_engine *e, const gft_graph *g, int32_t *d_label, const gft
         // outside it only.  An edge (v, w) skipped at v, which lies in the
         // giant component, is joined at w unless w lies there too: on a
         // symmetric graph every edge is also w's edge.
-        for (uint32_t r = 0; r < dev::kCcSampleEdges; r++) {
-            dev::cc_neighbour_round<<<blocks, block, 0, stream>>>(G.row_start, G.edge_dst, n, r, label, ctr);
-            GFT_CUDA_TRY(cudaGetLastError());
-            dev::cc_flatten<<<blocks, block, 0, stream>>>(label, n);
-            GFT_CUDA_TRY(cudaGetLastError());
-        }
+        dev::cc_neighbour_rounds<<<blocks, block, 0, stream>>>(G.row_start, G.edge_dst, n, label, ctr);
+        GFT_CUDA_TRY(cudaGetLastError());
+        dev::cc_flatten<<<blocks, block, 0, stream>>>(label, n);
+        GFT_CUDA_TRY(cudaGetLastError());
         dev::cc_sample_giant<<<1, dev::kCcSamples, 0, stream>>>(label, n, giant);
         GFT_CUDA_TRY(cudaGetLastError());
         dev::cc_hook<<<blocks, block, 0, stream>>>(G.row_start, G.edge_dst, n, label, hubs, hub_cap, 0,
@@ -312,7 +310,7 @@ gft_status run_cc(gft_engine *e, const gft_graph *g, int32_t *d_label, const gft
         float ms = 0;
         cudaEventElapsedTime(&ms, e->ev0, e->ev1);
         stats->levels = 1;
-        stats->iterations = G.symmetric ? 5 + 2 * dev::kCcSampleEdges : 4;  // kernel launches
+        stats->iterations = G.symmetric ? 7 : 4;  // kernel launches
         stats->vertices_reached = n;
         stats->edges_scanned = h[1];
         stats->kernel_ms = ms;
