@@ -7,8 +7,11 @@
 A step is one single-source query over a resident seeded graph.  The
 headline workload is SSSP on the 4096^2 road-like grid (16.8 M nodes, 5% of
 edges deleted, 0.1% shortcuts, weights uniform [1, 10000], seed 1, source
-drawn from the seed, delta 10000).  The metric is GTEPS = E_r / t, E_r the
-sum of out-degrees of the reached vertices.  Rank 0 prints one JSON line.
+drawn from the seed).  Its delta comes from the tuned parameters
+(galoisgpu_b200/tuned_b200.json, 40000; the reference's default is 10000):
+delta changes only the schedule, never the distances.  The metric is GTEPS =
+E_r / t, E_r the sum of out-degrees of the reached vertices.  Rank 0 prints
+one JSON line.
 
   value        device-resident throughput: K queries timed with CUDA events
                on the launching stream, max over ranks, all ranks' work summed
@@ -20,8 +23,11 @@ sum of out-degrees of the reached vertices.  Rank 0 prints one JSON line.
                against the measured HBM copy bandwidth
   cpu_baseline the CPU oracle (serial Dijkstra / FIFO BFS, one core) on the
                same query, rank 0 at N = 1 only; also checks bit-exact parity
-  secondary    BFS on RMAT-24 (64 seeded sources, harmonic-mean GTEPS) and on
-               the 256^2 grid, N = 1 only
+  secondary    N = 1 only: BFS on RMAT-24 (64 seeded sources, harmonic-mean
+               GTEPS) and on the 256^2 grid; 512 batched SSSP queries;
+               256-source BFS on RMAT-24; serving 8 resident graphs under
+               Poisson load; connected components on RMAT-24 and the road
+               grid (--workload cc-rmat-24 / cc-road-4096 runs one alone)
 
 --impl reference runs the reference arm: the reference has no CPU
 implementation of this path, so the oracle's restatement of it (kind
@@ -844,14 +850,33 @@ def main(argv=None) -> int:
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("gft", "reference"), default="gft")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS), default=HEADLINE)
+    ap.add_argument("--workload", choices=sorted(WORKLOADS) + sorted(CC_WORKLOADS), default=HEADLINE,
+                    help="a traversal workload (the headline by default) or a connected-components one")
     ap.add_argument("--no-secondary", action="store_true", help="skip the secondary workloads")
     args = ap.parse_args(argv)
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
     if args.impl == "reference":
         return reference_arm(args)
+    if args.workload in CC_WORKLOADS:
+        return cc_arm(args)
     return our_arm(args)
+
+
+def cc_arm(args) -> int:
+    """One connected-components workload on one GPU, as a JSON line."""
+    import torch
+
+    import galoisgpu_b200 as gft
+    from oracle import oracle as orc
+
+    torch.cuda.set_device(0)
+    r = bench_cc(gft, orc, args.workload, 0, steps=args.steps, warmup=args.warmup)
+    line = {**r, "n_gpus": 1, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+            "data": "synthetic: seeded graph generated on the device (SplitMix64 streams)",
+            "config": {"workload": args.workload, **CC_WORKLOADS[args.workload]}}
+    print(json.dumps(line), flush=True)
+    return 0
 
 
 if __name__ == "__main__":
