@@ -303,7 +303,7 @@ extern "C" {
 void gft_batch_destroy(gft_batch *b)
 {
     if (!b) return;
-    if (b->engine) cudaSetDevice(b->engine->device);
+    DeviceScope device_scope(b->engine ? b->engine->device : 0);
     if (b->exec) cudaGraphExecDestroy(b->exec);
     if (b->graph) cudaGraphDestroy(b->graph);
     if (b->capture_stream) cudaStreamDestroy(b->capture_stream);
@@ -355,7 +355,8 @@ gft_status gft_batch_create(gft_engine *e, const gft_query *q, uint32_t n, const
     });
     b->nbig = 0;
     for (uint32_t i = 0; i < n; i++) b->nbig += big(i);
-    cudaError_t err = cudaSetDevice(e->device);
+    DeviceScope device_scope(e->device);
+    cudaError_t err = device_scope.err;
     if (err == cudaSuccess) err = cudaMallocHost(&b->h_jobs, sizeof(BatchJob) * n);
     if (err != cudaSuccess) {
         gft_batch_destroy(b);
@@ -428,7 +429,8 @@ gft_status gft_batch_set_source(gft_batch *b, uint32_t query, uint32_t src)
 gft_status gft_batch_submit(gft_batch *b, void *stream)
 {
     if (!b) return fail(GFT_ERR_INVALID_ARG, "gft_batch_submit: batch is NULL");
-    GFT_CUDA_TRY(cudaSetDevice(b->engine->device));
+    DeviceScope device_scope(b->engine->device);
+    GFT_CUDA_TRY(device_scope.err);
     cudaStream_t s = (cudaStream_t)stream;
     GFT_CUDA_TRY(cudaEventRecord(b->ev0, s));
     GFT_CUDA_TRY(cudaGraphLaunch(b->exec, s));
@@ -440,7 +442,8 @@ gft_status gft_batch_submit(gft_batch *b, void *stream)
 gft_status gft_batch_wait(gft_batch *b, gft_query *q, gft_batch_stats *st)
 {
     if (!b) return fail(GFT_ERR_INVALID_ARG, "gft_batch_wait: batch is NULL");
-    GFT_CUDA_TRY(cudaSetDevice(b->engine->device));
+    DeviceScope device_scope(b->engine->device);
+    GFT_CUDA_TRY(device_scope.err);
     cudaStream_t s = b->last_stream;
     GFT_CUDA_TRY(cudaMemcpyAsync(b->h_jobs, b->d_jobs, sizeof(BatchJob) * b->n, cudaMemcpyDeviceToHost, s));
     GFT_CUDA_TRY(cudaStreamSynchronize(s));

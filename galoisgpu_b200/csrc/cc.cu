@@ -251,7 +251,8 @@ gft_status run_cc(gft_engine *e, const gft_graph *g, int32_t *d_label, const gft
     GFT_TRY(check_engine_graph(e, g));
     if (!d_label) return fail(GFT_ERR_INVALID_ARG, "gft_cc: label pointer is NULL");
     const DeviceGraph &G = g->g;
-    GFT_CUDA_TRY(cudaSetDevice(e->device));
+    DeviceScope device_scope(e->device);
+    GFT_CUDA_TRY(device_scope.err);
     const uint32_t n = G.nnodes;
     const uint32_t hub_cap = std::max<uint32_t>(1, std::min<uint64_t>(n, (uint64_t)G.nedges / dev::kCcHubDegree + 1));
     const size_t o_ctr = 0, o_err = 256, o_giant = 320, o_hubs = 512;

@@ -123,7 +123,8 @@ gft_status gft_engine_create(int device, gft_engine **out)
     *out = nullptr;
     int sms = 0, major = 0, minor = 0;
     GFT_TRY(device_ok(device, &sms, &major, &minor));
-    GFT_CUDA_TRY(cudaSetDevice(device));
+    DeviceScope device_scope(device);
+    GFT_CUDA_TRY(device_scope.err);
     gft_engine *e = new gft_engine();
     e->device = device;
     e->sms = sms;
@@ -145,7 +146,7 @@ gft_status gft_engine_create(int device, gft_engine **out)
 void gft_engine_destroy(gft_engine *e)
 {
     if (!e) return;
-    cudaSetDevice(e->device);
+    DeviceScope device_scope(e->device);
     e->scratch.release();
     e->ctl.release();
     e->aux.release();
@@ -168,7 +169,8 @@ gft_status gft_graph_upload(int device, const gft_csr *h, void *stream_, gft_gra
         return fail(GFT_ERR_INVALID_ARG, "gft_graph_upload: row_start[nnodes] != nedges");
     *out = nullptr;
     GFT_TRY(device_ok(device, nullptr, nullptr, nullptr));
-    GFT_CUDA_TRY(cudaSetDevice(device));
+    DeviceScope device_scope(device);
+    GFT_CUDA_TRY(device_scope.err);
     cudaStream_t stream = (cudaStream_t)stream_;
     gft_graph *g = new gft_graph();
     DeviceGraph &G = g->g;
@@ -209,8 +211,9 @@ gft_status gft_graph_wrap(int device, uint32_t nnodes, uint32_t nedges, const ui
     g->g.edge_dst = const_cast<uint32_t *>(d_edge_dst);
     g->g.edge_data = const_cast<int32_t *>(d_edge_data);
     g->g.wrapped = true;
-    gft_status st = cudaSetDevice(device) == cudaSuccess ? graph_degree_stats(g->g, nullptr)
-                                                           : fail(GFT_ERR_CUDA, "gft_graph_wrap: cudaSetDevice failed");
+    DeviceScope device_scope(device);
+    gft_status st = device_scope.err == cudaSuccess ? graph_degree_stats(g->g, nullptr)
+                                                    : fail(GFT_ERR_CUDA, "gft_graph_wrap: cudaSetDevice failed");
     if (st != GFT_OK) {
         delete g;
         return st;
@@ -257,7 +260,8 @@ gft_status gft_graph_download(const gft_graph *g, gft_csr *out)
     if (!g || !out) return fail(GFT_ERR_INVALID_ARG, "gft_graph_download: null argument");
     memset(out, 0, sizeof *out);
     const DeviceGraph &G = g->g;
-    GFT_CUDA_TRY(cudaSetDevice(G.device));
+    DeviceScope device_scope(G.device);
+    GFT_CUDA_TRY(device_scope.err);
     out->nnodes = G.nnodes;
     out->nedges = G.nedges;
     out->row_start = (uint32_t *)malloc(((size_t)G.nnodes + 1) * 4);
@@ -283,7 +287,8 @@ gft_status gft_graph_pick_sources(const gft_graph *g, uint64_t seed, uint32_t k,
 {
     if (!g || (k && !out_sources)) return fail(GFT_ERR_INVALID_ARG, "gft_graph_pick_sources: null argument");
     std::vector<uint32_t> rs((size_t)g->g.nnodes + 1);
-    GFT_CUDA_TRY(cudaSetDevice(g->g.device));
+    DeviceScope device_scope(g->g.device);
+    GFT_CUDA_TRY(device_scope.err);
     GFT_CUDA_TRY(cudaMemcpy(rs.data(), g->g.row_start, rs.size() * 4, cudaMemcpyDeviceToHost));
     return pick_sources_rs(g->g.nnodes, rs.data(), seed, k, out_sources);
 }
@@ -292,7 +297,7 @@ void gft_graph_free(gft_graph *g)
 {
     if (!g) return;
     if (!g->g.wrapped) {
-        cudaSetDevice(g->g.device);
+        DeviceScope device_scope(g->g.device);
         if (g->g.row_start) cudaFree(g->g.row_start);
         if (g->g.edge_dst) cudaFree(g->g.edge_dst);
         if (g->g.edge_data) cudaFree(g->g.edge_data);

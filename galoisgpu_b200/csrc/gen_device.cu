@@ -143,7 +143,8 @@ extern "C" gft_status gft_graph_generate(int device, const gft_gen_params *p, vo
     const uint64_t nkeys = 2 * npairs;
     if (nkeys >= 0x7FFFFFFFull) return fail(GFT_ERR_INVALID_ARG, "gft_graph_generate: too many edges for one sort");
 
-    GFT_CUDA_TRY(cudaSetDevice(device));
+    DeviceScope device_scope(device);
+    GFT_CUDA_TRY(device_scope.err);
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
     unsigned long long *k0 = nullptr, *k1 = nullptr;

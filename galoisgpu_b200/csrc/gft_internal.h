@@ -139,6 +139,25 @@ namespace gft {
 // Resolves tuning defaults and the cooperative grid for a kernel.
 gft_status resolve_shape(gft_engine *e, const void *kernel, int block_threads, int blocks_per_sm,
                          size_t dyn_smem, LaunchShape *out);
+// Makes `device` current for one entry point and gives the caller's current
+// device back when the scope ends, so no call leaves the calling thread on
+// another device.
+struct DeviceScope {
+    int prev = -1;
+    cudaError_t err = cudaSuccess;
+    explicit DeviceScope(int device)
+    {
+        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+        err = cudaSetDevice(device);
+    }
+    ~DeviceScope()
+    {
+        if (prev >= 0) cudaSetDevice(prev);
+    }
+    DeviceScope(const DeviceScope &) = delete;
+    DeviceScope &operator=(const DeviceScope &) = delete;
+};
+
 // Largest out-degree of a device graph, stored in G.max_degree (one small
 // reduction kernel on `stream`, then a wait).
 gft_status graph_degree_stats(DeviceGraph &G, cudaStream_t stream);

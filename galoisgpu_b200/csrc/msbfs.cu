@@ -405,7 +405,8 @@ gft_status gft_msbfs(gft_engine *e, const gft_graph *g, const uint32_t *h_source
     for (uint32_t i = 0; i < k; i++)
         if (h_sources[i] >= G.nnodes) return fail(GFT_ERR_INVALID_ARG, "gft_msbfs: source %u out of range", i);
     cudaStream_t stream = (cudaStream_t)stream_;
-    GFT_CUDA_TRY(cudaSetDevice(e->device));
+    DeviceScope device_scope(e->device);
+    GFT_CUDA_TRY(device_scope.err);
     const uint32_t WP = row_words(k);
     const size_t vwords = (size_t)G.nnodes * WP;
     auto a256 = [](size_t x) { return (x + 255) & ~(size_t)255; };

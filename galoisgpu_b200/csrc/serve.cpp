@@ -323,7 +323,8 @@ gft_status gft_serve_open(gft_engine *e, const gft_serve_config *cfg_in, gft_ser
         s->cfg.max_lanes_per_request = s->cfg.lanes;
     if (s->cfg.wide_lanes == GFT_SERVE_AUTO) s->cfg.wide_lanes = s->cfg.lanes >= 4 ? (s->cfg.lanes * 4 + 8) / 9 : 0;
     if (s->cfg.wide_lanes >= s->cfg.lanes) s->cfg.wide_lanes = s->cfg.lanes - 1;
-    cudaError_t err = cudaSetDevice(e->device);
+    DeviceScope device_scope(e->device);
+    cudaError_t err = device_scope.err;
     s->lanes.resize(s->cfg.lanes);
     for (auto &l : s->lanes) {
         if (err == cudaSuccess) err = cudaStreamCreateWithFlags(&l.stream, cudaStreamNonBlocking);
@@ -403,7 +404,7 @@ gft_status gft_serve_close(gft_server *s)
     }
     s->cv_work.notify_all();
     if (s->dispatcher.joinable()) s->dispatcher.join();
-    cudaSetDevice(s->engine->device);
+    DeviceScope device_scope(s->engine->device);
     for (auto &l : s->lanes) {
         if (l.stream) cudaStreamSynchronize(l.stream);
         if (l.stream) cudaStreamDestroy(l.stream);

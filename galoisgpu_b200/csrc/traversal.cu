@@ -259,7 +259,8 @@ gft_status run_traversal(bool is_sssp, gft_engine *e, const gft_graph *g, uint32
     const void *kern = is_sssp ? sssp_kernel_for(t.block) : bfs_kernel_for(t.block);
     if (!kern) return fail(GFT_ERR_INVALID_ARG, "%s: block_threads must be 256, 512 or 1024", what);
     if (t.hub < 32) t.hub = 32;
-    GFT_CUDA_TRY(cudaSetDevice(e->device));
+    DeviceScope device_scope(e->device);
+    GFT_CUDA_TRY(device_scope.err);
     // One CTA for small graphs (max_blocks 0 = automatic) or on request
     // (max_blocks 1); the whole cooperative grid otherwise.
     const bool single = t.max_blocks == 1 || (t.max_blocks == 0 && t.skip < 0 && G.nnodes <= kCtaMaxNodes &&
@@ -352,7 +353,8 @@ gft_status run_traversal(bool is_sssp, gft_engine *e, const gft_graph *g, uint32
 gft_status reach_stats(const gft_graph *g, const int32_t *d_val, cudaStream_t stream, uint64_t *v_r, uint64_t *e_r)
 {
     unsigned long long *d = nullptr, h[2] = {0, 0};
-    GFT_CUDA_TRY(cudaSetDevice(g->g.device));
+    DeviceScope device_scope(g->g.device);
+    GFT_CUDA_TRY(device_scope.err);
     GFT_CUDA_TRY(cudaMallocAsync(&d, 16, stream));
     GFT_CUDA_TRY(cudaMemsetAsync(d, 0, 16, stream));
     dev::reach_stats_kernel<<<592, 256, 0, stream>>>(g->g.row_start, d_val, g->g.nnodes, d);
@@ -501,7 +503,8 @@ extern "C" gft_status gft_bfs_noalloc(const gft_graph *g, uint32_t src, int32_t 
     uint32_t hub = (tune && tune->hub_degree) ? std::max<uint32_t>(tune->hub_degree, 32) : 4096;
     uint32_t timeout_ms = (tune && tune->timeout_ms) ? tune->timeout_ms : 20000;
     cudaStream_t stream = (cudaStream_t)stream_;
-    GFT_CUDA_TRY(cudaSetDevice(G.device));
+    DeviceScope device_scope(G.device);
+    GFT_CUDA_TRY(device_scope.err);
     char *base = nullptr;
     GFT_TRY(noalloc_scratch(G.device, &base));
 
