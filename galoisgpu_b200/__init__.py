@@ -1,6 +1,6 @@
 """galoisgpu_b200 -- B200 (sm_100a) frontier-traversal engine for the
-data-driven worklist BFS and SSSP path of LonestarGPU v3, and connected
-components (apps/cc) on the same engine.
+data-driven worklist BFS and SSSP path of LonestarGPU v3, with connected
+components (apps/cc) and PageRank (apps/pr) on the same engine.
 
 The compute lives in libgft.so (hand-written CUDA for sm_100a behind the C
 ABI of include/gft.h); this package is the Python host side.
@@ -18,6 +18,7 @@ from .graph import (  # noqa: F401
     output,
     reach_stats,
     write_cc_output,
+    write_pr_output,
 )
 from ._lib import GftError, load  # noqa: F401
 

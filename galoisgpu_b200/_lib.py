@@ -196,6 +196,9 @@ _SIGS: dict[str, tuple] = {
     "gft_cc": (C.c_int, [_P, _P, _P, C.POINTER(Tuning), _P, C.POINTER(Stats), C.POINTER(C.c_uint64)]),
     "gft_cc_host": (C.c_int, [_P, _P, _P, C.POINTER(Tuning), _P, C.POINTER(Stats), C.POINTER(C.c_uint64)]),
     "gft_write_cc_output": (C.c_int, [C.c_char_p, C.POINTER(Csr), _P]),
+    "gft_pr": (C.c_int, [_P, _P, _P, C.c_uint32, C.POINTER(Tuning), _P, C.POINTER(Stats)]),
+    "gft_pr_host": (C.c_int, [_P, _P, _P, C.c_uint32, C.POINTER(Tuning), _P, C.POINTER(Stats)]),
+    "gft_write_pr_output": (C.c_int, [C.c_char_p, C.c_uint32, _P]),
     "gft_bfs_noalloc": (C.c_int, [_P, C.c_uint32, _P, _P, C.POINTER(Tuning), _P, C.POINTER(Stats)]),
     "gft_write_output": (C.c_int, [C.c_char_p, C.c_uint32, _P]),
     "gft_batch_create": (C.c_int, [_P, C.POINTER(Query), C.c_uint32, C.POINTER(Tuning), C.POINTER(_P)]),

@@ -3,11 +3,13 @@
 //   bfs  [-q] [-g gpunum] [-o output-file] [-l] [-s startNode] graph-file
 //   sssp [-q] [-g gpunum] [-o output-file] [-l] [-d delta] [-s startNode] graph-file
 //   cc   [-q] [-g gpunum] [-o output-file] graph-file
+//   pr   [-q] [-g gpunum] [-o output-file] [-n] [-t top_ranks] [-x max_iterations] graph-file
 //
 // Same options, same stdout/stderr lines and same output file as the
 // reference driver (skelapp/skel.cu:37-151 with apps/bfs/support.cu:5-45,
-// apps/sssp/support.cu:6-53 and apps/cc/support.cu:3-36; cc prints the
-// reference's "components: N" line, apps/cc/kernel.cu:719).  CC labels are
+// apps/sssp/support.cu:6-53, apps/cc/support.cu:3-36 and apps/pr/support.cu:
+// 15-104; cc prints the reference's "components: N" line, apps/cc/kernel.cu:
+// 719, and pr its "PR took N iterations" and "sum: S (N)" lines).  CC labels are
 // the smallest vertex id of each component, where the reference's are
 // whichever roots its racy hooks leave: the partition is the same.  The traversal runs through the C ABI.  `-l`
 // (the reference's host-driven load balancer, apps/bfs/kernel.cu:286-311) is
@@ -25,16 +27,21 @@
 
 #include "gft.h"
 
-// The app this binary is: 0 bfs, 1 sssp, 2 cc (set by the build).
+// The app this binary is: 0 bfs, 1 sssp, 2 cc, 3 pr (set by the build).
 #ifndef GFT_CLI_APP
 #define GFT_CLI_APP 0
 #endif
 #define GFT_CLI_SSSP (GFT_CLI_APP == 1)
 #define GFT_CLI_CC (GFT_CLI_APP == 2)
+#define GFT_CLI_PR (GFT_CLI_APP == 3)
 
-static const char *kAppOpts = GFT_CLI_CC ? "" : GFT_CLI_SSSP ? "ls:d:" : "ls:";
-static const char *kAppUsage = GFT_CLI_CC ? "" : GFT_CLI_SSSP ? "[-l] [-d delta] [-s startNode]" : "[-l] [-s startNode]";
-static const char *kAppArgsUsage = GFT_CLI_CC ? "" : "-l: enable thread block load balancer (by default false)";
+static const char *kAppOpts = GFT_CLI_PR ? "nt:x:" : GFT_CLI_CC ? "" : GFT_CLI_SSSP ? "ls:d:" : "ls:";
+static const char *kAppUsage = GFT_CLI_PR   ? "[-n] [-t top_ranks] [-x max_iterations]"
+                               : GFT_CLI_CC ? ""
+                               : GFT_CLI_SSSP ? "[-l] [-d delta] [-s startNode]"
+                                              : "[-l] [-s startNode]";
+static const char *kAppArgsUsage =
+    (GFT_CLI_CC || GFT_CLI_PR) ? "" : "-l: enable thread block load balancer (by default false)";
 
 static void usage(const char *argv0)
 {
@@ -61,7 +68,8 @@ int main(int argc, char **argv)
         usage(argv[0]);
         return 1;
     }
-    int quiet = 0, device = 0, start_node = 0, delta = 10000;
+    int quiet = 0, device = 0, start_node = 0, delta = 10000, no_print_rank = 0;
+    uint32_t max_iterations = 0xFFFFFFFFu;
     const char *output = nullptr;
     char opts[32];
     snprintf(opts, sizeof opts, "g:qo:%s", kAppOpts);
@@ -94,6 +102,9 @@ int main(int argc, char **argv)
             }
             break;
         case 'l': break;
+        case 'n': no_print_rank = 1; break;
+        case 't': break;  // accepted: the reference's output ignores it (apps/pr/support.cu:83-94)
+        case 'x': max_iterations = (uint32_t)strtoul(optarg, nullptr, 10); break;
         default: usage(argv[0]); return EXIT_FAILURE;
         }
     }
@@ -104,14 +115,15 @@ int main(int argc, char **argv)
     const char *input = argv[optind];
 
     fprintf(stderr, "OPTIONS: gft engine (libgft %d, sm_100a %s)\n", gft_version(),
-            GFT_CLI_CC ? "union-find CC" : GFT_CLI_SSSP ? "persistent near-far SSSP" : "persistent BFS");
+            GFT_CLI_PR ? "persistent residual-push PageRank" : GFT_CLI_CC ? "union-find CC"
+            : GFT_CLI_SSSP ? "persistent near-far SSSP" : "persistent BFS");
     gft_csr h;
     uint64_t t0 = now_ns();
     gft_status s = gft_gr_read(input, &h);
     if (s != GFT_OK) return die("read", s);
     printf("nnodes=%u, nedges=%u.\n", h.nnodes, h.nedges);
     printf("read %s in %llu ms\n", input, (unsigned long long)((now_ns() - t0) / 1000000));
-    if (!GFT_CLI_CC && (uint32_t)start_node >= h.nnodes) {
+    if (!GFT_CLI_CC && !GFT_CLI_PR && (uint32_t)start_node >= h.nnodes) {
         fprintf(stderr, "start node %d out of range (%u nodes)\n", start_node, h.nnodes);
         gft_csr_free(&h);
         return EXIT_FAILURE;
@@ -126,8 +138,11 @@ int main(int argc, char **argv)
     gft_stats st;
     memset(&st, 0, sizeof st);
     uint64_t comps = 0;
+    std::vector<float> rank(GFT_CLI_PR ? h.nnodes : 0);
     uint64_t k0 = now_ns();
-    if (GFT_CLI_CC) {
+    if (GFT_CLI_PR) {
+        s = gft_pr_host(e, g, rank.data(), max_iterations, nullptr, nullptr, &st);
+    } else if (GFT_CLI_CC) {
         s = gft_cc_host(e, g, val.data(), nullptr, nullptr, &st, &comps);
     } else if (GFT_CLI_SSSP) {
         printf("delta: %d\n", delta);
@@ -136,7 +151,8 @@ int main(int argc, char **argv)
         s = gft_bfs_host(e, g, (uint32_t)start_node, val.data(), nullptr, nullptr, nullptr, &st);
     }
     uint64_t k1 = now_ns();
-    if (s != GFT_OK) return die(GFT_CLI_CC ? "cc" : GFT_CLI_SSSP ? "sssp" : "bfs", s);
+    if (s != GFT_OK) return die(GFT_CLI_PR ? "pr" : GFT_CLI_CC ? "cc" : GFT_CLI_SSSP ? "sssp" : "bfs", s);
+    if (GFT_CLI_PR) printf("PR took %u iterations\n", st.levels);
     if (GFT_CLI_SSSP) printf("iterations: %u\n", st.levels);
     if (GFT_CLI_CC) printf("components: %llu\n", (unsigned long long)comps);
     printf("gg_main %llu %llu\n", (unsigned long long)k0, (unsigned long long)k1);
@@ -145,8 +161,30 @@ int main(int argc, char **argv)
     fprintf(stderr, "Kernel time: %.3f ms (%u levels/phases, %u grid iterations)\n", st.kernel_ms, st.levels,
             st.iterations);
     int rc = 0;
+    if (GFT_CLI_PR && !quiet) {  // apps/pr/support.cu:56-65: a float sum in node order
+        fprintf(stderr, "Calculating sum ...\n");
+        float sum = 0;
+        for (uint32_t i = 0; i < h.nnodes; i++) sum += rank[i];
+        fprintf(stdout, "sum: %f (%d)\n", (double)sum, (int)h.nnodes);
+    }
     if (!quiet && output) {
-        s = GFT_CLI_CC ? gft_write_cc_output(output, &h, val.data()) : gft_write_output(output, h.nnodes, val.data());
+        if (GFT_CLI_PR && no_print_rank) {
+            FILE *f = strcmp(output, "-") == 0 ? stdout : fopen(output, "w");
+            if (!f) {
+                fprintf(stderr, "output: cannot open %s\n", output);
+                rc = 1;
+            } else {
+                for (uint32_t i = 0; i < h.nnodes; i++) fprintf(f, "%d\n", (int)i);
+                if (f != stdout) fclose(f);
+            }
+            s = GFT_OK;
+        } else if (GFT_CLI_PR) {
+            s = gft_write_pr_output(output, h.nnodes, rank.data());
+        } else if (GFT_CLI_CC) {
+            s = gft_write_cc_output(output, &h, val.data());
+        } else {
+            s = gft_write_output(output, h.nnodes, val.data());
+        }
         if (s != GFT_OK) rc = die("output", s);
     }
     gft_engine_destroy(e);

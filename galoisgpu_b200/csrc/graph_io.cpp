@@ -321,4 +321,37 @@ gft_status gft_write_cc_output(const char *path, const gft_csr *g, const int32_t
     return GFT_OK;
 }
 
+gft_status gft_write_pr_output(const char *path, uint32_t nnodes, const float *h_rank)
+{
+    if (!path || (nnodes && !h_rank)) return fail(GFT_ERR_INVALID_ARG, "gft_write_pr_output: null argument");
+    bool to_stdout = strcmp(path, "-") == 0;
+    FILE *f = to_stdout ? stdout : fopen(path, "w");
+    if (!f) return fail(GFT_ERR_IO, "gft_write_pr_output: cannot open %s: %s", path, strerror(errno));
+    // "%d %f\n" per node, node order (apps/pr/support.cu:95-101); formatted in
+    // parallel blocks, written in order.
+    const uint32_t block = 1u << 20;
+    uint32_t nblocks = (nnodes + block - 1) / block;
+    bool ok = true;
+    unsigned nt = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+    for (uint32_t b0 = 0; b0 < nblocks && ok; b0 += nt) {
+        uint32_t nb = std::min<uint32_t>(nt, nblocks - b0);
+        std::vector<std::string> text(nb);
+        std::vector<std::thread> th;
+        for (uint32_t t = 0; t < nb; t++)
+            th.emplace_back([&, t] {
+                uint32_t lo = (b0 + t) * block, hi = std::min<uint32_t>(nnodes, lo + block);
+                std::string &s = text[t];
+                s.reserve((size_t)(hi - lo) * 20);
+                char line[64];
+                for (uint32_t i = lo; i < hi; i++) s.append(line, snprintf(line, sizeof line, "%d %f\n", (int)i, (double)h_rank[i]));
+            });
+        for (auto &x : th) x.join();
+        for (auto &s : text) ok = ok && write_all(f, s.data(), s.size());
+    }
+    if (to_stdout) fflush(f);
+    else if (fclose(f) != 0) ok = false;
+    if (!ok) return fail(GFT_ERR_IO, "gft_write_pr_output: write to %s failed", path);
+    return GFT_OK;
+}
+
 }  // extern "C"

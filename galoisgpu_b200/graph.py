@@ -396,6 +396,29 @@ class Engine:
                                  _stream_ptr(stream), C.byref(st), C.byref(comps)))
         return {"components": comps.value, **st.as_dict()}
 
+    def pr(self, graph: DeviceGraph, out=None, max_iterations: int = 0xFFFFFFFF, tune: Tune | None = None,
+           stream=None) -> dict:
+        """PageRank by residual push (apps/pr): ``out`` (float32 device tensor)
+        receives the unnormalised ranks; ``levels`` = worklist rounds run."""
+        import torch
+
+        dev = torch.device("cuda", graph.device)
+        if out is None:
+            out = torch.empty(graph.nnodes, dtype=torch.float32, device=dev)
+        st = Stats()
+        check(load().gft_pr(self._h, graph.handle, C.c_void_p(out.data_ptr()), max_iterations, self._tune(tune),
+                            _stream_ptr(stream if stream is not None else torch.cuda.current_stream(dev)),
+                            C.byref(st)))
+        return {"out": out, **st.as_dict()}
+
+    def pr_host(self, graph: DeviceGraph, out: np.ndarray, max_iterations: int = 0xFFFFFFFF,
+                tune: Tune | None = None, stream=None) -> dict:
+        """PageRank into a host float32 array (end to end)."""
+        st = Stats()
+        check(load().gft_pr_host(self._h, graph.handle, C.c_void_p(out.ctypes.data), max_iterations,
+                                 self._tune(tune), _stream_ptr(stream), C.byref(st)))
+        return st.as_dict()
+
     def bfs_host(self, graph: DeviceGraph, start_node: int, out: np.ndarray, parent: np.ndarray | None = None,
                  tune: Tune | None = None, stream=None) -> dict:
         """End-to-end query with host result buffers (int32 / uint32 numpy)."""
@@ -512,6 +535,13 @@ def write_cc_output(path: str | Path, graph: CSRGraph, labels: np.ndarray) -> No
     check(load().gft_write_cc_output(str(path).encode(), C.byref(c), C.c_void_p(lab.ctypes.data)))
 
 
+def write_pr_output(path: str | Path, ranks: np.ndarray) -> None:
+    """Ranks as the reference writes them: "%d %f" per node
+    (apps/pr/support.cu:95-101)."""
+    r = np.ascontiguousarray(ranks, dtype=np.float32)
+    check(load().gft_write_pr_output(str(path).encode(), len(r), C.c_void_p(r.ctypes.data)))
+
+
 __all__ = [
     "Batch",
     "CSRGraph",
@@ -524,5 +554,6 @@ __all__ = [
     "reach_stats",
     "output",
     "write_cc_output",
+    "write_pr_output",
     "_lib",
 ]

@@ -409,6 +409,23 @@ GFT_API gft_status gft_cc_host(gft_engine *e, const gft_graph *g, int32_t *h_lab
  * CSR supplies the edges.  path "-" writes to stdout. */
 GFT_API gft_status gft_write_cc_output(const char *path, const gft_csr *g, const int32_t *h_label);
 
+/* ---------------------------------------------------------------------------
+ * PageRank by residual push: replaces apps/pr gg_main (apps/pr/kernel.cu:
+ * 362-389) with its constants ALPHA = 0.85 and EPSILON = 1e-6 (:19-20).
+ * d_rank (float, nnodes entries) receives the unnormalised ranks the
+ * reference prints; max_iterations bounds the worklist rounds (its -x
+ * option; UINT32_MAX = until converged); stats->levels = rounds run.  Float
+ * atomicAdd makes the summation order, and so the last bits of the ranks,
+ * depend on the schedule, in the reference as here.
+ * ------------------------------------------------------------------------- */
+GFT_API gft_status gft_pr(gft_engine *e, const gft_graph *g, float *d_rank, uint32_t max_iterations,
+                          const gft_tuning *tune, void *stream, gft_stats *stats);
+GFT_API gft_status gft_pr_host(gft_engine *e, const gft_graph *g, float *h_rank, uint32_t max_iterations,
+                               const gft_tuning *tune, void *stream, gft_stats *stats);
+/* Writes ranks as the reference does: "%d %f\n" per node (apps/pr/support.cu:
+ * 95-101).  path "-" writes to stdout. */
+GFT_API gft_status gft_write_pr_output(const char *path, uint32_t nnodes, const float *h_rank);
+
 /* Reach statistics of a result already on the device: V_r (vertices with a
  * finite value) and E_r (sum of their out-degrees, the edges a top-down
  * traversal must scan).  Waits for `stream`. */

@@ -23,6 +23,10 @@
  *                                 endpoints), :449-462 (a component is a
  *                                 vertex that is its own label),
  *                                 apps/cc/support.cu:16-36 (output)
+ *   - PageRank (residual push)    apps/pr/kernel.cu:17-20 (ALPHA, EPSILON),
+ *                                 :26-47 (init_1), :49-63 (init_2),
+ *                                 :127-236 (pop and push), :271-305 (driver),
+ *                                 apps/pr/support.cu:47-104 (output)
  *
  * The reference's BFS and SSSP results are schedule independent: BFS levels
  * are hop distances and SSSP distances are the unique shortest-path lengths
@@ -35,6 +39,11 @@
  * components is not, and neither is the count.  This restatement labels
  * every vertex with the smallest vertex id of its component; parity with the
  * reference is checked on the partition.
+ *
+ * PageRank accumulates float residuals with atomicAdd in whatever order the
+ * GPU runs, so its ranks are not bit-reproducible even between two runs of
+ * the reference; this restatement processes each level of its worklist in
+ * vertex order with the same float arithmetic, and parity is a tolerance.
  *
  * Parity of this restatement is pinned against outputs of the reference's
  * own CUDA build (oracle/ref/Makefile builds it from the reference sources;
@@ -327,5 +336,74 @@ int orc_write_cc_output(const char *path, uint32_t nnodes, const uint32_t *row_s
             fprintf(f, "\te %d: %d %d %d\n", j, (int)d, edge_data ? edge_data[j] : 0, label[d]);
         }
     }
+    return fclose(f) ? -2 : 0;
+}
+
+/* ------------------------------------------------------------------ */
+/* PageRank by residual push (apps/pr/kernel.cu).  Constants and the    */
+/* mixed float/double arithmetic of the reference:                      */
+/*   rank[v]  = 1.0 - ALPHA                          (init_1, :37)      */
+/*   res[dst] += (float)(1.0 / outdeg(v)) per edge    (:38-45)           */
+/*   res[v]  *= (1.0 - ALPHA) * ALPHA, in double      (init_2, :60)      */
+/* then every vertex is in the first worklist, and each worklist vertex */
+/* u takes r = res[u], res[u] = 0, rank[u] += r, and pushes             */
+/* r * ALPHA / outdeg(u) to each neighbour; a neighbour whose residual  */
+/* crosses EPSILON from below joins the next worklist (:140-143,        */
+/* :184-192).  Worklists are processed level by level, each in order.  */
+/* Returns the number of iterations (worklists processed).              */
+/* ------------------------------------------------------------------ */
+#define ORC_PR_ALPHA 0.85f
+#define ORC_PR_EPSILON 0.000001f
+
+int64_t orc_pr(uint32_t nnodes, const uint32_t *row_start, const uint32_t *edge_dst, int64_t max_iterations,
+               float *rank)
+{
+    float *res = (float *)calloc(nnodes ? nnodes : 1, sizeof(float));
+    uint32_t *cur = (uint32_t *)malloc((size_t)(nnodes ? nnodes : 1) * 4);
+    uint32_t *nxt = (uint32_t *)malloc((size_t)(nnodes ? nnodes : 1) * 4);
+    for (uint32_t v = 0; v < nnodes; v++) rank[v] = (float)(1.0 - (double)ORC_PR_ALPHA);
+    for (uint32_t v = 0; v < nnodes; v++) {
+        uint32_t deg = row_start[v + 1] - row_start[v];
+        if (!deg) continue;
+        float upd = (float)(1.0 / deg);
+        for (uint32_t e = row_start[v]; e < row_start[v + 1]; e++) res[edge_dst[e]] += upd;
+    }
+    for (uint32_t v = 0; v < nnodes; v++)
+        res[v] = (float)((double)res[v] * ((1.0 - (double)ORC_PR_ALPHA) * (double)ORC_PR_ALPHA));
+    size_t ncur = 0;
+    for (uint32_t v = 0; v < nnodes; v++) cur[ncur++] = v;
+    int64_t iter = 0;
+    while (ncur && iter < max_iterations) {
+        size_t nn = 0;
+        for (size_t i = 0; i < ncur; i++) {
+            uint32_t u = cur[i];
+            float r = res[u];
+            res[u] = 0;
+            rank[u] += r;
+            uint32_t deg = row_start[u + 1] - row_start[u];
+            if (!deg) continue;
+            float upd = r * ORC_PR_ALPHA / (float)deg;
+            for (uint32_t e = row_start[u]; e < row_start[u + 1]; e++) {
+                uint32_t d = edge_dst[e];
+                float prev = res[d];
+                float now = prev + upd;
+                res[d] = now;
+                if (now > ORC_PR_EPSILON && prev < ORC_PR_EPSILON) nxt[nn++] = d;
+            }
+        }
+        uint32_t *t = cur; cur = nxt; nxt = t;
+        ncur = nn;
+        iter++;
+    }
+    free(res); free(cur); free(nxt);
+    return iter;
+}
+
+/* PageRank output (apps/pr/support.cu:95-101): "%d %f\n" per node. */
+int orc_write_pr_output(const char *path, uint32_t nnodes, const float *rank)
+{
+    FILE *f = fopen(path, "w");
+    if (!f) return -1;
+    for (int i = 0; i < (int)nnodes; i++) fprintf(f, "%d %f\n", i, (double)rank[i]);
     return fclose(f) ? -2 : 0;
 }

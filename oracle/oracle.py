@@ -53,6 +53,10 @@ def load():
         lib.orc_read_output.argtypes = [C.c_char_p, C.c_uint32, C.c_void_p]
         lib.orc_cc.restype = C.c_uint64
         lib.orc_cc.argtypes = [C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p]
+        lib.orc_pr.restype = C.c_int64
+        lib.orc_pr.argtypes = [C.c_uint32, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p]
+        lib.orc_write_pr_output.restype = C.c_int
+        lib.orc_write_pr_output.argtypes = [C.c_char_p, C.c_uint32, C.c_void_p]
         lib.orc_write_cc_output.restype = C.c_int
         lib.orc_write_cc_output.argtypes = [C.c_char_p, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
         _lib = lib
@@ -173,3 +177,30 @@ def canonical_labels(label) -> np.ndarray:
     first = np.full(max(n, int(lab.max()) + 1 if n else 0), n, dtype=np.int64)
     np.minimum.at(first, lab, np.arange(n, dtype=np.int64))
     return first[lab].astype(np.int32)
+
+
+def pr(row_start, edge_dst, max_iterations: int = 2**62) -> tuple[np.ndarray, int]:
+    """PageRank by residual push: (float32 rank per vertex, iterations)."""
+    rs = np.ascontiguousarray(row_start, dtype=np.uint32)
+    dst = np.ascontiguousarray(edge_dst, dtype=np.uint32)
+    n = len(rs) - 1
+    rank = np.empty(max(n, 1), dtype=np.float32)[:n]
+    it = load().orc_pr(n, _p(rs), _p(dst), max_iterations, _p(rank))
+    return rank, int(it)
+
+
+def write_pr_output(path, rank) -> None:
+    r = np.ascontiguousarray(rank, dtype=np.float32)
+    rc = load().orc_write_pr_output(str(path).encode(), len(r), _p(r))
+    if rc != 0:
+        raise OSError(f"orc_write_pr_output({path}) failed: {rc}")
+
+
+def read_pr_output(path, nnodes: int) -> np.ndarray:
+    """Ranks from a reference PageRank output file ("%d %f" lines)."""
+    rank = np.full(nnodes, np.nan, dtype=np.float64)
+    with open(path) as f:
+        for ln in f:
+            i, v = ln.split()
+            rank[int(i)] = float(v)
+    return rank

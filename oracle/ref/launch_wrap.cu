@@ -4,7 +4,8 @@
  *
  * 1. Cooperative launch of the persistent drivers.
  * The reference's persistent drivers gg_main_pipe_N_gpu_gb
- * (apps/bfs/kernel.cu:375, apps/sssp/kernel.cu:448, apps/cc/kernel.cu:481,569)
+ * (apps/bfs/kernel.cu:375, apps/sssp/kernel.cu:448, apps/cc/kernel.cu:481,569,
+ * apps/pr/kernel.cu:271)
  * synchronise their CTAs
  * with a software grid barrier that spins without a limit
  * (rt/include/gbar.cuh:84-120), sized by a hand-written occupancy table
@@ -46,7 +47,7 @@ extern "C" cudaError_t __wrap_cudaLaunchKernel(const void *func, dim3 grid, dim3
         long long padded = (long long)*size * 4 + (4ll << 20);  // ints in the padded dwl allocation
         *size = (int)(padded > 0x7FFFFFFFll ? 0x7FFFFFFFll : padded);
     }
-    if (name && strstr(name, "_gpu_gb")) {  // gg_main_pipe_N_gpu_gb: bfs, sssp, cc
+    if (name && strstr(name, "_gpu_gb")) {  // gg_main_pipe_N_gpu_gb: bfs, sssp, cc, pr
         cudaError_t e = cudaLaunchCooperativeKernel(func, grid, block, args, smem, stream);
         if (e != cudaSuccess)
             fprintf(stderr, "oracle-ref: cooperative launch of %s (%u x %u) refused: %s\n", name, grid.x,
