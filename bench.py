@@ -26,8 +26,9 @@ one JSON line.
   secondary    N = 1 only: BFS on RMAT-24 (64 seeded sources, harmonic-mean
                GTEPS) and on the 256^2 grid; 512 batched SSSP queries;
                256-source BFS on RMAT-24; serving 8 resident graphs under
-               Poisson load; connected components on RMAT-24 and the road
-               grid (--workload cc-rmat-24 / cc-road-4096 runs one alone)
+               Poisson load; connected components and PageRank on RMAT-24
+               and the road grid (--workload cc-rmat-24, pr-road-4096, ...
+               runs one alone)
 
 --impl reference runs the reference arm: the reference has no CPU
 implementation of this path, so the oracle's restatement of it (kind
@@ -468,6 +469,12 @@ def our_arm(args) -> int:
                 sec["serve-8-graphs"] = bench_serve(gft, dev)
             except Exception as ex:
                 sec["serve-8-graphs"] = {"error": repr(ex)}
+            for pname in PR_WORKLOADS:
+                try:
+                    torch.cuda.empty_cache()
+                    sec[pname] = bench_pr(gft, orc, pname, dev)
+                except Exception as ex:
+                    sec[pname] = {"error": repr(ex)}
             for cname in CC_WORKLOADS:
                 try:
                     torch.cuda.empty_cache()
@@ -543,6 +550,78 @@ def bench_cc(gft, orc, name: str, dev: int, steps: int = 10, warmup: int = 3) ->
     }
     log(f"[{name}] {res['value']:.1f} GTEPS, kernel {kernel_ms:.3f} ms, {r['components']} components, "
         f"parity {res['parity_vs_oracle']}")
+    eng.close()
+    dg.free()
+    return res
+
+
+PR_WORKLOADS = {
+    "pr-rmat-24": dict(kind="rmat", scale=24, edge_factor=16, seed=1),
+    "pr-road-4096": dict(kind="road", side=4096, seed=1),
+}
+
+
+def bench_pr(gft, orc, name: str, dev: int, steps: int = 5, warmup: int = 3, cpu_seconds: float = 10.0) -> dict:
+    """PageRank by residual push (apps/pr on this engine) to convergence on a
+    full-size seeded graph: GTEPS = edges pushed / kernel time, end to end
+    with the ranks copied to pinned host memory, and the oracle on one host
+    core, capped at the iterations that fit in about cpu_seconds (its
+    per-edge rate is the CPU baseline; the ranks are checked against the
+    oracle in the tests, at sizes the oracle finishes in seconds)."""
+    import torch
+
+    spec = {**PR_WORKLOADS[name], "app": "pr"}
+    dg = make_device_graph(gft, spec, dev)
+    eng = gft.Engine(dev)
+    out = torch.empty(dg.nnodes, dtype=torch.float32, device=f"cuda:{dev}")
+    stream = torch.cuda.current_stream(dev)
+    for _ in range(warmup):
+        r = eng.pr(dg, out=out, stream=stream)
+    torch.cuda.synchronize(dev)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    runs = [eng.pr(dg, out=out, stream=stream) for _ in range(steps)]
+    ev1.record(stream)
+    torch.cuda.synchronize(dev)
+    total_ms = ev0.elapsed_time(ev1) / steps
+    kernel_ms = statistics.mean(x["kernel_ms"] for x in runs)
+    pushed = statistics.mean(x["edges_scanned"] for x in runs)
+    h_out = torch.empty(dg.nnodes, dtype=torch.float32, pin_memory=True).numpy()
+    t1 = time.perf_counter()
+    for _ in range(steps):
+        eng.pr_host(dg, h_out)
+    e2e_s = (time.perf_counter() - t1) / steps
+    host = dg.download()
+    cpu = {}
+    iters = 1
+    while True:  # grow the capped oracle run until it takes about cpu_seconds
+        t2 = time.perf_counter()
+        orc.pr(host.row_start, host.edge_dst, max_iterations=iters, stats=cpu)
+        dt = time.perf_counter() - t2
+        if dt * 2 > cpu_seconds or iters >= runs[0]["levels"]:
+            break
+        iters *= 2
+    peak, peak_kind = measured_peaks()
+    pops = statistics.mean(x["pushes"] for x in runs)
+    # Bytes a push step must move per edge pushed: its destination (4 B), the
+    # residual read-modify-write (8 B); per worklist entry popped: the entry,
+    # the residual exchange, the rank update and the row pair (20 B).
+    alg = 12 * pushed + 20 * pops
+    res = {
+        "metric": "GTEPS (edges pushed)", "value": pushed / (total_ms * 1e6), "unit": "GTEPS",
+        "kernel_ms_mean": kernel_ms, "iterations": runs[0]["levels"], "edges_pushed": pushed, "pops": pops,
+        "steps": steps,
+        "warmup": warmup, "nodes": dg.nnodes, "edges": dg.nedges,
+        "e2e": {"value": pushed / (e2e_s * 1e9), "unit": "GTEPS", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": dg.nnodes * 4},
+        "roofline": {"bound": "hbm", "achieved": alg / (kernel_ms * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
+                     "frac": alg / (kernel_ms * 1e-3) / 1e9 / peak, "traffic": None, "peak_kind": peak_kind,
+                     "alg_bytes_per_launch": alg, "kernel": "pr_persistent"},
+        "cpu_baseline": {"value": cpu["edges_pushed"] / dt / 1e9, "unit": "GTEPS", "cores": 1, "kind": "port",
+                         "sample": f"the oracle's first {iters} iterations ({cpu['edges_pushed']} edges pushed, "
+                                   f"{dt:.1f} s)"},
+    }
+    log(f"[{name}] {res['value']:.1f} GTEPS, kernel {kernel_ms:.3f} ms, {runs[0]['levels']} iterations")
     eng.close()
     dg.free()
     return res
@@ -850,31 +929,35 @@ def main(argv=None) -> int:
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("gft", "reference"), default="gft")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS) + sorted(CC_WORKLOADS), default=HEADLINE,
-                    help="a traversal workload (the headline by default) or a connected-components one")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS) + sorted(CC_WORKLOADS) + sorted(PR_WORKLOADS),
+                    default=HEADLINE, help="a traversal workload (the headline by default), or a connected-components "
+                                           "or PageRank one")
     ap.add_argument("--no-secondary", action="store_true", help="skip the secondary workloads")
     args = ap.parse_args(argv)
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
     if args.impl == "reference":
         return reference_arm(args)
-    if args.workload in CC_WORKLOADS:
+    if args.workload in CC_WORKLOADS or args.workload in PR_WORKLOADS:
         return cc_arm(args)
     return our_arm(args)
 
 
 def cc_arm(args) -> int:
-    """One connected-components workload on one GPU, as a JSON line."""
+    """One connected-components or PageRank workload on one GPU, as a JSON
+    line."""
     import torch
 
     import galoisgpu_b200 as gft
     from oracle import oracle as orc
 
     torch.cuda.set_device(0)
-    r = bench_cc(gft, orc, args.workload, 0, steps=args.steps, warmup=args.warmup)
-    line = {**r, "n_gpus": 1, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+    is_pr = args.workload in PR_WORKLOADS
+    r = (bench_pr if is_pr else bench_cc)(gft, orc, args.workload, 0, steps=args.steps, warmup=args.warmup)
+    line = {**r, "n_gpus": 1, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32" if is_pr else "u32",
             "data": "synthetic: seeded graph generated on the device (SplitMix64 streams)",
-            "config": {"workload": args.workload, **CC_WORKLOADS[args.workload]}}
+            "config": {"workload": args.workload, **(PR_WORKLOADS if is_pr else CC_WORKLOADS)[args.workload]}}
     print(json.dumps(line), flush=True)
     return 0
 

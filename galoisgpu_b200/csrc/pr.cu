@@ -135,6 +135,10 @@ struct PrVisitor {
         for (int k = 0; k < K; k++) {
             cross[k] = false;
             if (valid[k]) {
+                // The reference's crossing test (apps/pr/kernel.cu:190,222).
+                // A sum that rounds to exactly EPSILON passes neither half,
+                // and that vertex is never queued again: its later residual
+                // never reaches its rank, in the reference as here.
                 const float prev = atomicAdd(residual + d[k], o[k].upd);
                 cross[k] = prev + o[k].upd > kPrEpsilon && prev < kPrEpsilon;
                 edges++;
@@ -240,10 +244,12 @@ __global__ void __launch_bounds__(BLOCK, 2048 / BLOCK) pr_persistent(PrParams pp
     vis.q.err_where = &ctl->error_where;
 
     unsigned L = 0;
+    unsigned long long pops = 0;  // worklist entries processed (thread 0's tally)
     for (;;) {
         const unsigned slot = L % 3, nslot = (L + 1) % 3, rslot = (L + 2) % 3;
         const unsigned n_in = m.ld(u32_of(ctl->qlen[slot]));
         if (n_in == 0 || L >= pp.max_iterations) break;
+        pops += n_in;
         if (tid == 0) {
             *u32_of(ctl->qlen[rslot]) = 0;
             *u32_of(ctl->claim[rslot]) = 0;
@@ -272,6 +278,7 @@ __global__ void __launch_bounds__(BLOCK, 2048 / BLOCK) pr_persistent(PrParams pp
     if (tid == 0) {
         ctl->levels = L;
         ctl->iterations = m.epoch();
+        ctl->pushes = pops;
     }
 }
 
@@ -361,6 +368,7 @@ gft_status run_pr(gft_engine *e, const gft_graph *g, float *d_rank, uint32_t max
         stats->iterations = h->iterations;
         stats->vertices_reached = n;
         stats->edges_scanned = h->edges;
+        stats->pushes = h->pushes;
         stats->kernel_ms = ms;
         stats->grid_blocks = shape.blocks;
         stats->block_threads = shape.block_threads;

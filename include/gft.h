@@ -414,7 +414,9 @@ GFT_API gft_status gft_write_cc_output(const char *path, const gft_csr *g, const
  * 362-389) with its constants ALPHA = 0.85 and EPSILON = 1e-6 (:19-20).
  * d_rank (float, nnodes entries) receives the unnormalised ranks the
  * reference prints; max_iterations bounds the worklist rounds (its -x
- * option; UINT32_MAX = until converged); stats->levels = rounds run.  Float
+ * option; UINT32_MAX = until converged); stats->levels = rounds run,
+ * stats->edges_scanned = edges pushed along, stats->pushes = worklist
+ * entries processed over all rounds.  Float
  * atomicAdd makes the summation order, and so the last bits of the ranks,
  * depend on the schedule, in the reference as here.
  * ------------------------------------------------------------------------- */

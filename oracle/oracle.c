@@ -350,14 +350,16 @@ int orc_write_cc_output(const char *path, uint32_t nnodes, const uint32_t *row_s
 /* r * ALPHA / outdeg(u) to each neighbour; a neighbour whose residual  */
 /* crosses EPSILON from below joins the next worklist (:140-143,        */
 /* :184-192).  Worklists are processed level by level, each in order.  */
-/* Returns the number of iterations (worklists processed).              */
+/* Returns the number of iterations (worklists processed); the edges   */
+/* pushed along go to *edges_pushed when it is not NULL.                */
 /* ------------------------------------------------------------------ */
 #define ORC_PR_ALPHA 0.85f
 #define ORC_PR_EPSILON 0.000001f
 
 int64_t orc_pr(uint32_t nnodes, const uint32_t *row_start, const uint32_t *edge_dst, int64_t max_iterations,
-               float *rank)
+               float *rank, uint64_t *edges_pushed)
 {
+    uint64_t pushed = 0;
     float *res = (float *)calloc(nnodes ? nnodes : 1, sizeof(float));
     uint32_t *cur = (uint32_t *)malloc((size_t)(nnodes ? nnodes : 1) * 4);
     uint32_t *nxt = (uint32_t *)malloc((size_t)(nnodes ? nnodes : 1) * 4);
@@ -383,6 +385,7 @@ int64_t orc_pr(uint32_t nnodes, const uint32_t *row_start, const uint32_t *edge_
             uint32_t deg = row_start[u + 1] - row_start[u];
             if (!deg) continue;
             float upd = r * ORC_PR_ALPHA / (float)deg;
+            pushed += deg;
             for (uint32_t e = row_start[u]; e < row_start[u + 1]; e++) {
                 uint32_t d = edge_dst[e];
                 float prev = res[d];
@@ -396,6 +399,7 @@ int64_t orc_pr(uint32_t nnodes, const uint32_t *row_start, const uint32_t *edge_
         iter++;
     }
     free(res); free(cur); free(nxt);
+    if (edges_pushed) *edges_pushed = pushed;
     return iter;
 }
 

@@ -54,7 +54,7 @@ def load():
         lib.orc_cc.restype = C.c_uint64
         lib.orc_cc.argtypes = [C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p]
         lib.orc_pr.restype = C.c_int64
-        lib.orc_pr.argtypes = [C.c_uint32, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p]
+        lib.orc_pr.argtypes = [C.c_uint32, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.POINTER(C.c_uint64)]
         lib.orc_write_pr_output.restype = C.c_int
         lib.orc_write_pr_output.argtypes = [C.c_char_p, C.c_uint32, C.c_void_p]
         lib.orc_write_cc_output.restype = C.c_int
@@ -179,13 +179,17 @@ def canonical_labels(label) -> np.ndarray:
     return first[lab].astype(np.int32)
 
 
-def pr(row_start, edge_dst, max_iterations: int = 2**62) -> tuple[np.ndarray, int]:
-    """PageRank by residual push: (float32 rank per vertex, iterations)."""
+def pr(row_start, edge_dst, max_iterations: int = 2**62, stats: dict | None = None) -> tuple[np.ndarray, int]:
+    """PageRank by residual push: (float32 rank per vertex, iterations); the
+    edges pushed along go to stats["edges_pushed"] when stats is given."""
     rs = np.ascontiguousarray(row_start, dtype=np.uint32)
     dst = np.ascontiguousarray(edge_dst, dtype=np.uint32)
     n = len(rs) - 1
     rank = np.empty(max(n, 1), dtype=np.float32)[:n]
-    it = load().orc_pr(n, _p(rs), _p(dst), max_iterations, _p(rank))
+    pushed = C.c_uint64()
+    it = load().orc_pr(n, _p(rs), _p(dst), max_iterations, _p(rank), C.byref(pushed))
+    if stats is not None:
+        stats["edges_pushed"] = pushed.value
     return rank, int(it)
 
 

@@ -1,13 +1,15 @@
 """Times the reference's own CUDA build (oracle/_ref, built by
 oracle/ref/Makefile from the reference sources) on the full-size seeded
 configurations, the way a user runs it: ``bfs|sssp -q -s <src> [-d delta]
-<graph.gr>`` or ``cc -q <graph.gr>``, one process per query, reading its
+<graph.gr>``, ``cc -q <graph.gr>`` or ``pr -q <graph.gr>``, one process per
+query, reading its
 ``Total time: N ns`` line
 (reference skelapp/skel.cu:159-166; that time includes the worklist
 allocations gg_main makes, apps/bfs/kernel.cu:389, apps/sssp/kernel.cu:475).
 Kernel-only time comes from running this same script under
 ``ncu --metrics gpu__time_duration.sum -k regex:gg_main_pipe`` (for cc, every
-kernel of the process: its driver is a host loop of launches).
+kernel of the process: its driver is a host loop of launches; for pr the
+init kernels and the persistent gg_main_pipe_1_gpu_gb).
 
 Test/measurement infrastructure only: the input graphs are produced with this
 repository's generator, and E_r comes from this repository's engine (whose
@@ -46,7 +48,41 @@ CONFIGS = {
     "rmat20": dict(kind="rmat", kw=dict(scale=20, edge_factor=16), seed=1, app="bfs", src_seed=2),
     "cc-rmat24": dict(kind="rmat", kw=dict(scale=24, edge_factor=16), seed=1, app="cc", src_seed=None),
     "cc-road4096": dict(kind="road", kw=dict(side=4096), seed=1, app="cc", src_seed=None),
+    "pr-rmat24": dict(kind="rmat", kw=dict(scale=24, edge_factor=16), seed=1, app="pr", src_seed=None),
+    "pr-road4096": dict(kind="road", kw=dict(side=4096), seed=1, app="pr", src_seed=None),
 }
+
+
+def run_pr(a, c, dg, host, eng, gr: Path) -> int:
+    """The reference's PageRank to convergence against this engine's: total
+    time, iterations, and with --check the largest rank difference (float
+    atomics make neither side bit-reproducible)."""
+    mine = eng.pr(dg)
+    cmd = [str(REF / "pr")]
+    out = Path(a.workdir) / f"gft_{a.config}.pr.out"
+    cmd += ["-o", str(out)] if a.check else ["-q"]
+    t = time.time()
+    r = subprocess.run(cmd + [str(gr)], capture_output=True, text=True, timeout=1800)
+    wall = time.time() - t
+    if r.returncode != 0:
+        print(r.stdout, r.stderr, file=sys.stderr)
+        return r.returncode
+    m = re.search(r"Total time: (\d+) ns", r.stderr)
+    ns = int(m.group(1)) if m else None
+    it = int(re.search(r"PR took (\d+) iterations", r.stdout).group(1))
+    rec = {"config": a.config, "app": "pr", "total_time_ns": ns, "iterations": it, "edges": dg.nedges,
+           "gft_kernel_ms": mine["kernel_ms"], "gft_iterations": mine["levels"],
+           "gft_edges_pushed": mine["edges_scanned"], "process_wall_s": wall}
+    if a.check:
+        ref = orc.read_pr_output(out, host.nnodes)
+        got = mine["out"].cpu().numpy()
+        err = np.abs(got - ref) / np.maximum(1.0, np.abs(ref))
+        rec["max_rel_diff_vs_gft"] = float(err.max())
+        rec["vertices_over_1e-4"] = int(np.count_nonzero(err > 1e-4))
+        out.unlink()
+    print(json.dumps(rec), flush=True)
+    gr.unlink()
+    return 0
 
 
 def main(argv=None) -> int:
@@ -70,6 +106,8 @@ def main(argv=None) -> int:
     eng = gft.Engine(0)
     delta = a.delta or c.get("delta")
     results = []
+    if c["app"] == "pr":
+        return run_pr(a, c, dg, host, eng, gr)
     if c["app"] == "cc":
         # Component count only: the reference's CC output lists every edge
         # (apps/cc/support.cu:30-35), about 15 GB of text for RMAT-24.

