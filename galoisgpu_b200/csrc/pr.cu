@@ -13,13 +13,20 @@
 // until the worklist is empty (:271-305).  Here the same steps run in one
 // persistent cooperative launch on the frontier machinery of frontier.cuh:
 // the per-vertex expansion tiers (flattened, warp, grid-wide hubs), the
-// warp-aggregated queue, and the bounded grid barrier.  A vertex joins the
-// next worklist at most once per iteration (a per-vertex stamp), so every
-// vertex is popped by exactly one thread per iteration and its rank needs no
-// atomic; the reference may list a vertex twice, and the second pop then
-// finds whatever residual arrived in between, which here waits for the next
-// iteration instead.  Float atomicAdd makes the summation order, and so the
-// last bits of the ranks, depend on the schedule, as in the reference.
+// warp-aggregated queue, and the bounded grid barrier.
+//
+// One rule differs, for the hardware: the worklist of the next round is every
+// vertex whose residual exceeds EPSILON when the round ends, collected by a
+// sweep of the residuals after the round's barrier, instead of the vertices
+// whose residual crossed EPSILON during a push.  A push then needs no return
+// value, so it is a fire-and-forget float reduction in L2 instead of an
+// atomic whose result the warp waits for (the crossing test).  Each vertex
+// is listed once, so it has one popper per round and its rank needs no
+// atomic.  Two consequences: a residual that rounds to exactly EPSILON, which
+// the reference's crossing test never queues again (its later residual never
+// reaches its rank), is picked up once it grows; and at the end every
+// residual is at most EPSILON.  Float addition in schedule order makes the
+// last bits of the ranks run-dependent, as in the reference.
 #include <string.h>
 
 #include <algorithm>
@@ -96,17 +103,17 @@ struct PrInitVisitor {
 };
 
 // One push step.  owner() pops the vertex (its only side effect), except in
-// the hub phase, where the hub's update was stored when it was popped.
+// the hub phase, where the hub's update was stored when it was popped.  A
+// push is a float add whose result is not used (a fire-and-forget reduction
+// in L2): the next worklist is built after the round from the residuals
+// themselves, so no push waits for the residual it changed.
 struct PrVisitor {
     static constexpr int kBatch = 2;
     const uint32_t *__restrict__ row_start;
     const uint32_t *__restrict__ edge_dst;
     float *rank, *residual, *hub_upd;
-    uint32_t *stamp;
-    uint32_t next_stamp;  // this iteration's push stamp
     uint32_t hub_degree;
     bool hub_phase;
-    WarpQueue q;
     unsigned long long edges;
     bool vec;
 
@@ -115,7 +122,7 @@ struct PrVisitor {
         if (!has) return PrOwn{u, 0.f};
         if (hub_phase) return PrOwn{u, __ldcg(hub_upd + u)};
         const float r = __uint_as_float(atomicExch(reinterpret_cast<unsigned *>(residual + u), 0u));
-        rank[u] += r;  // one popper per vertex per iteration
+        rank[u] += r;  // a worklist lists a vertex once: one popper per round
         const uint32_t deg = __ldg(row_start + u + 1) - __ldg(row_start + u);
         const float upd = deg ? r * kPrAlpha / (float)deg : 0.f;
         if (deg >= hub_degree) hub_upd[u] = upd;
@@ -127,37 +134,18 @@ struct PrVisitor {
         return PrOwn{__shfl_sync(kFull, o.u, lane), __shfl_sync(kFull, o.upd, lane)};
     }
     template <int K>
-    __device__ __forceinline__ void pushK(const bool (&valid)[K], const uint32_t (&d)[K], const PrOwn (&o)[K],
-                                          unsigned lane)
-    {
-        bool cross[K];
-#pragma unroll
-        for (int k = 0; k < K; k++) {
-            cross[k] = false;
-            if (valid[k]) {
-                // The reference's crossing test (apps/pr/kernel.cu:190,222).
-                // A sum that rounds to exactly EPSILON passes neither half,
-                // and that vertex is never queued again: its later residual
-                // never reaches its rank, in the reference as here.
-                const float prev = atomicAdd(residual + d[k], o[k].upd);
-                cross[k] = prev + o[k].upd > kPrEpsilon && prev < kPrEpsilon;
-                edges++;
-            }
-        }
-#pragma unroll
-        for (int k = 0; k < K; k++) {
-            const bool push = cross[k] && atomicExch(stamp + d[k], next_stamp) != next_stamp;
-            q.push(push, d[k], lane);
-        }
-    }
-    template <int K>
     __device__ __forceinline__ void edgeK(const bool (&valid)[K], const uint32_t (&e)[K], const PrOwn (&o)[K],
                                           unsigned lane)
     {
         uint32_t d[K];
 #pragma unroll
         for (int k = 0; k < K; k++) d[k] = valid[k] ? __ldcs(edge_dst + e[k]) : 0u;
-        pushK<K>(valid, d, o, lane);
+#pragma unroll
+        for (int k = 0; k < K; k++)
+            if (valid[k]) {
+                atomicAdd(residual + d[k], o[k].upd);  // result unused: a reduction
+                edges++;
+            }
     }
     __device__ __forceinline__ void edge1(bool valid, uint32_t e, const PrOwn &o, unsigned lane)
     {
@@ -169,19 +157,36 @@ struct PrVisitor {
     __device__ __forceinline__ void edge4(bool valid, uint32_t e, const PrOwn &o, unsigned lane)
     {
         const uint4 x = valid ? __ldcs(reinterpret_cast<const uint4 *>(edge_dst + e)) : make_uint4(0, 0, 0, 0);
-        const bool v[4] = {valid, valid, valid, valid};
-        const uint32_t d[4] = {x.x, x.y, x.z, x.w};
-        const PrOwn oo[4] = {o, o, o, o};
-        pushK<4>(v, d, oo, lane);
+        if (valid) {
+            atomicAdd(residual + x.x, o.upd);
+            atomicAdd(residual + x.y, o.upd);
+            atomicAdd(residual + x.z, o.upd);
+            atomicAdd(residual + x.w, o.upd);
+            edges += 4;
+        }
     }
 };
 
 struct PrParams {
     TravParams t;  // graph, queues, hubs, control block (expansion machinery)
     float *rank, *residual, *hub_upd;
-    uint32_t *stamp;
     uint32_t max_iterations;
 };
+
+// Appends every vertex whose residual exceeds EPSILON to the next worklist
+// (each vertex once, so a worklist never lists a vertex twice).  Runs between
+// two grid barriers, when no push is in flight.
+__device__ __forceinline__ void pr_collect(const float *residual, uint32_t n, WarpQueue &q, unsigned gwarp,
+                                           unsigned nwarps, unsigned lane)
+{
+    for (uint32_t base = gwarp * 32u; base < n; base += nwarps * 32u) {
+        const uint32_t v = base + lane;
+        const bool has = v < n;
+        const float r = has ? __ldcg(residual + v) : 0.f;
+        q.push(has && r > kPrEpsilon, v, lane);
+    }
+    q.flush(lane);
+}
 
 template <int BLOCK>
 __global__ void __launch_bounds__(BLOCK, 2048 / BLOCK) pr_persistent(PrParams pp)
@@ -200,7 +205,6 @@ __global__ void __launch_bounds__(BLOCK, 2048 / BLOCK) pr_persistent(PrParams pp
     for (uint32_t v = tid; v < n; v += nthreads) {
         pp.rank[v] = (float)(1.0 - (double)kPrAlpha);
         pp.residual[v] = 0.f;
-        pp.stamp[v] = 0;
         p.q[0][v] = v;
     }
     if (tid == 0) *u32_of(ctl->qlen[0]) = n;
@@ -232,17 +236,19 @@ __global__ void __launch_bounds__(BLOCK, 2048 / BLOCK) pr_persistent(PrParams pp
     vis.rank = pp.rank;
     vis.residual = pp.residual;
     vis.hub_upd = pp.hub_upd;
-    vis.stamp = pp.stamp;
     vis.hub_degree = p.hub_degree;
     vis.hub_phase = false;
     vis.edges = 0;
     vis.vec = p.vec_ok != 0;
-    vis.q.buf = s_buf[threadIdx.x >> 5];
-    vis.q.count = 0;
-    vis.q.cap = p.qcap;
-    vis.q.err = &ctl->error;
-    vis.q.err_where = &ctl->error_where;
+    WarpQueue q;
+    q.buf = s_buf[threadIdx.x >> 5];
+    q.count = 0;
+    q.cap = p.qcap;
+    q.err = &ctl->error;
+    q.err_where = &ctl->error_where;
 
+    // Round L: pop and push the worklist Q(L) (its hubs in a grid-wide second
+    // phase), then collect Q(L+1) from the residuals.
     unsigned L = 0;
     unsigned long long pops = 0;  // worklist entries processed (thread 0's tally)
     for (;;) {
@@ -256,22 +262,21 @@ __global__ void __launch_bounds__(BLOCK, 2048 / BLOCK) pr_persistent(PrParams pp
             ctl->hub[rslot].v = 0;
             *u32_of(ctl->hub_claim[rslot]) = 0;
         }
-        vis.q.queue = sel2(p.q, (L + 1));
-        vis.q.len = u32_of(ctl->qlen[nslot]);
-        vis.next_stamp = L + 1;
         vis.hub_phase = false;
         expand_frontier<PrVisitor, PrOwn>(vis, p, sel2(p.q, L), n_in, u32_of(ctl->claim[slot]), &ctl->hub[slot].v,
                                           pick_grain(n_in, nwarps, p.uniform), gwarp, nwarps, lane);
-        vis.q.flush(lane);
         if (!m.sync()) return;
         const unsigned long long hv = m.ld64(&ctl->hub[slot].v);
         if (hv) {
             vis.hub_phase = true;
             expand_hubs<PrVisitor, PrOwn>(vis, p, (unsigned)(hv >> 32), (unsigned)hv, u32_of(ctl->hub_claim[slot]),
                                           gwarp, nwarps, lane);
-            vis.q.flush(lane);
             if (!m.sync()) return;
         }
+        q.queue = sel2(p.q, (L + 1));
+        q.len = u32_of(ctl->qlen[nslot]);
+        pr_collect(pp.residual, n, q, gwarp, nwarps, lane);
+        if (!m.sync()) return;
         L++;
     }
     warp_add_u64(&ctl->edges, vis.edges, lane);
@@ -322,7 +327,7 @@ gft_status run_pr(gft_engine *e, const gft_graph *g, float *d_rank, uint32_t max
         return o;
     };
     const size_t o_q0 = take((size_t)n * 4), o_q1 = take((size_t)n * 4), o_hubs = take((size_t)hub_cap * 8),
-                 o_res = take((size_t)n * 4), o_upd = take((size_t)n * 4), o_stamp = take((size_t)n * 4);
+                 o_res = take((size_t)n * 4), o_upd = take((size_t)n * 4);
     GFT_TRY(e->scratch.ensure(off));
     char *base = static_cast<char *>(e->scratch.ptr);
     dev::PrParams pp{};
@@ -345,7 +350,6 @@ gft_status run_pr(gft_engine *e, const gft_graph *g, float *d_rank, uint32_t max
     pp.rank = d_rank;
     pp.residual = reinterpret_cast<float *>(base + o_res);
     pp.hub_upd = reinterpret_cast<float *>(base + o_upd);
-    pp.stamp = reinterpret_cast<uint32_t *>(base + o_stamp);
     pp.max_iterations = max_iterations;
     GFT_CUDA_TRY(cudaMemsetAsync(e->ctl.ptr, 0, sizeof(TraversalCtl), stream));
     void *args[] = {&pp};

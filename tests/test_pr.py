@@ -10,15 +10,18 @@ tolerance used throughout is |a - b| <= RTOL * max(1, |b|), RTOL = 1e-4: the
 largest relative difference between the oracle and the reference on the
 golden graphs is 5.2e-5, on the 5000-leaf star whose hub holds rank 2298.
 
-A few vertices per run may miss RTOL for a second reason, also the
-reference's: its crossing test `prev + update > EPSILON && prev < EPSILON`
+A few vertices per run may miss RTOL for a second reason, the reference's:
+its crossing test `prev + update > EPSILON && prev < EPSILON`
 (apps/pr/kernel.cu:190,222) fails when a residual sum rounds to exactly
 EPSILON, and that vertex is never queued again, so the residual it gathers
 afterwards never reaches its rank.  Which vertex lands there depends on the
-summation order: 0-4 per run on the 32768-vertex R-MAT below, on the GPU as in
-shuffled sequential schedules.  Such a vertex falls short by what it gathers
-in the remaining iterations, a few 1e-5 relative.  So up to MAX_STUCK vertices
-per graph may miss RTOL, and they must still be within LOOSE_RTOL."""
+summation order: 0-4 per run on the 32768-vertex R-MAT below in shuffled
+sequential schedules of the oracle (which restates that test).  Such a vertex
+falls short by what it gathers in the remaining rounds, a few 1e-5 relative.
+gft_pr builds each worklist from the residuals above EPSILON instead, so it
+has no such vertex, but the oracle and the golden ranks may.  So up to
+MAX_STUCK vertices per graph may miss RTOL, and they must still be within
+LOOSE_RTOL."""
 
 import json
 import re
