@@ -40,6 +40,13 @@ namespace dev {
 constexpr float kPrAlpha = 0.85f;       // apps/pr/kernel.cu:19
 constexpr float kPrEpsilon = 0.000001f;  // apps/pr/kernel.cu:20
 
+// Float add to global memory with no return value (a reduction performed in
+// L2): the issuing warp does not wait for it.
+__device__ __forceinline__ void red_add_f32(float *p, float v)
+{
+    asm volatile("red.relaxed.gpu.global.add.f32 [%0], %1;" ::"l"(p), "f"(v) : "memory");
+}
+
 struct PrOwn {
     uint32_t u;
     float upd;  // what each of u's edges adds to its destination's residual
@@ -72,7 +79,7 @@ struct PrInitVisitor {
 #pragma unroll
         for (int k = 0; k < K; k++)
             if (valid[k]) {
-                atomicAdd(residual + d[k], o[k].upd);
+                red_add_f32(residual + d[k], o[k].upd);
                 edges++;
             }
     }
@@ -108,7 +115,7 @@ struct PrInitVisitor {
 // in L2): the next worklist is built after the round from the residuals
 // themselves, so no push waits for the residual it changed.
 struct PrVisitor {
-    static constexpr int kBatch = 2;
+    static constexpr int kBatch = 4;
     const uint32_t *__restrict__ row_start;
     const uint32_t *__restrict__ edge_dst;
     float *rank, *residual, *hub_upd;
@@ -143,7 +150,7 @@ struct PrVisitor {
 #pragma unroll
         for (int k = 0; k < K; k++)
             if (valid[k]) {
-                atomicAdd(residual + d[k], o[k].upd);  // result unused: a reduction
+                red_add_f32(residual + d[k], o[k].upd);
                 edges++;
             }
     }
@@ -158,10 +165,10 @@ struct PrVisitor {
     {
         const uint4 x = valid ? __ldcs(reinterpret_cast<const uint4 *>(edge_dst + e)) : make_uint4(0, 0, 0, 0);
         if (valid) {
-            atomicAdd(residual + x.x, o.upd);
-            atomicAdd(residual + x.y, o.upd);
-            atomicAdd(residual + x.z, o.upd);
-            atomicAdd(residual + x.w, o.upd);
+            red_add_f32(residual + x.x, o.upd);
+            red_add_f32(residual + x.y, o.upd);
+            red_add_f32(residual + x.z, o.upd);
+            red_add_f32(residual + x.w, o.upd);
             edges += 4;
         }
     }
