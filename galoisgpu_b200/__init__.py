@@ -1,6 +1,7 @@
 """galoisgpu_b200 -- B200 (sm_100a) frontier-traversal engine for the
 data-driven worklist BFS and SSSP path of LonestarGPU v3, with connected
-components (apps/cc) and PageRank (apps/pr) on the same engine.
+components (apps/cc), PageRank (apps/pr) and maximal independent set
+(apps/mis) on the same engine.
 
 The compute lives in libgft.so (hand-written CUDA for sm_100a behind the C
 ABI of include/gft.h); this package is the Python host side.
@@ -19,6 +20,7 @@ from .graph import (  # noqa: F401
     reach_stats,
     write_cc_output,
     write_pr_output,
+    write_mis_output,
 )
 from ._lib import GftError, load  # noqa: F401
 

@@ -199,6 +199,9 @@ _SIGS: dict[str, tuple] = {
     "gft_pr": (C.c_int, [_P, _P, _P, C.c_uint32, C.POINTER(Tuning), _P, C.POINTER(Stats)]),
     "gft_pr_host": (C.c_int, [_P, _P, _P, C.c_uint32, C.POINTER(Tuning), _P, C.POINTER(Stats)]),
     "gft_write_pr_output": (C.c_int, [C.c_char_p, C.c_uint32, _P]),
+    "gft_mis": (C.c_int, [_P, _P, _P, C.c_uint32, C.POINTER(Tuning), _P, C.POINTER(Stats)]),
+    "gft_mis_host": (C.c_int, [_P, _P, _P, C.c_uint32, C.POINTER(Tuning), _P, C.POINTER(Stats)]),
+    "gft_write_mis_output": (C.c_int, [C.c_char_p, C.c_uint32, _P]),
     "gft_bfs_noalloc": (C.c_int, [_P, C.c_uint32, _P, _P, C.POINTER(Tuning), _P, C.POINTER(Stats)]),
     "gft_write_output": (C.c_int, [C.c_char_p, C.c_uint32, _P]),
     "gft_batch_create": (C.c_int, [_P, C.POINTER(Query), C.c_uint32, C.POINTER(Tuning), C.POINTER(_P)]),

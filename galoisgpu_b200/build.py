@@ -3,7 +3,7 @@
 Compiles every CUDA source for sm_100a only (``-gencode
 arch=compute_100a,code=sm_100a -lineinfo``) and the host sources with g++,
 then links ``galoisgpu_b200/libgft.so`` (CUDA runtime linked statically) and
-``galoisgpu_b200/bin/{bfs,sssp,cc,pr}``.  Objects go to ``galoisgpu_b200/_build``;
+``galoisgpu_b200/bin/{bfs,sssp,cc,pr,mis}``.  Objects go to ``galoisgpu_b200/_build``;
 unchanged sources are not recompiled.
 
     python -m galoisgpu_b200.build [--force] [--verbose]
@@ -42,6 +42,7 @@ LIB_SOURCES = [
     "serve.cpp",
     "cc.cu",
     "pr.cu",
+    "mis.cu",
 ]
 HEADERS = ["gft_internal.h", "gen_common.h", "traverse.cuh", "frontier.cuh"]
 CLI_SOURCE = "cli_main.cpp"
@@ -123,7 +124,7 @@ def build(force: bool = False, verbose: bool = False, ptxas_verbose: bool = Fals
         os.replace(tmp, LIB)
     cli_src = CSRC / CLI_SOURCE
     if cli_src.exists():
-        for app_id, app in enumerate(("bfs", "sssp", "cc", "pr")):
+        for app_id, app in enumerate(("bfs", "sssp", "cc", "pr", "mis")):
             cli_obj = BUILD / f"cli_{app}.o"
             if force or _newer(cli_obj, [cli_src, INCLUDE / "gft.h"]):
                 _run(["g++", *CXX_FLAGS, f"-DGFT_CLI_APP={app_id}", "-c", str(cli_src), "-o",

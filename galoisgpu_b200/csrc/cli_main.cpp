@@ -4,12 +4,15 @@
 //   sssp [-q] [-g gpunum] [-o output-file] [-l] [-d delta] [-s startNode] graph-file
 //   cc   [-q] [-g gpunum] [-o output-file] graph-file
 //   pr   [-q] [-g gpunum] [-o output-file] [-n] [-t top_ranks] [-x max_iterations] graph-file
+//   mis  [-q] [-g gpunum] [-o output-file] graph-file
 //
 // Same options, same stdout/stderr lines and same output file as the
 // reference driver (skelapp/skel.cu:37-151 with apps/bfs/support.cu:5-45,
-// apps/sssp/support.cu:6-53, apps/cc/support.cu:3-36 and apps/pr/support.cu:
-// 15-104; cc prints the reference's "components: N" line, apps/cc/kernel.cu:
-// 719, and pr its "PR took N iterations" and "sum: S (N)" lines).  CC labels are
+// apps/sssp/support.cu:6-53, apps/cc/support.cu:3-36, apps/pr/support.cu:
+// 15-104 and apps/mis/support.cu:1-40; cc prints the reference's
+// "components: N" line, apps/cc/kernel.cu:719, pr its "PR took N iterations"
+// and "sum: S (N)" lines, and mis its "Total steps: N" line,
+// apps/mis/kernel.cu:231).  CC labels are
 // the smallest vertex id of each component, where the reference's are
 // whichever roots its racy hooks leave: the partition is the same.  The traversal runs through the C ABI.  `-l`
 // (the reference's host-driven load balancer, apps/bfs/kernel.cu:286-311) is
@@ -27,21 +30,23 @@
 
 #include "gft.h"
 
-// The app this binary is: 0 bfs, 1 sssp, 2 cc, 3 pr (set by the build).
+// The app this binary is: 0 bfs, 1 sssp, 2 cc, 3 pr, 4 mis (set by the build).
 #ifndef GFT_CLI_APP
 #define GFT_CLI_APP 0
 #endif
 #define GFT_CLI_SSSP (GFT_CLI_APP == 1)
 #define GFT_CLI_CC (GFT_CLI_APP == 2)
 #define GFT_CLI_PR (GFT_CLI_APP == 3)
+#define GFT_CLI_MIS (GFT_CLI_APP == 4)
+#define GFT_CLI_NO_SOURCE (GFT_CLI_CC || GFT_CLI_PR || GFT_CLI_MIS)
 
-static const char *kAppOpts = GFT_CLI_PR ? "nt:x:" : GFT_CLI_CC ? "" : GFT_CLI_SSSP ? "ls:d:" : "ls:";
+static const char *kAppOpts = GFT_CLI_PR ? "nt:x:" : (GFT_CLI_CC || GFT_CLI_MIS) ? "" : GFT_CLI_SSSP ? "ls:d:" : "ls:";
 static const char *kAppUsage = GFT_CLI_PR   ? "[-n] [-t top_ranks] [-x max_iterations]"
-                               : GFT_CLI_CC ? ""
+                               : (GFT_CLI_CC || GFT_CLI_MIS) ? ""
                                : GFT_CLI_SSSP ? "[-l] [-d delta] [-s startNode]"
                                               : "[-l] [-s startNode]";
 static const char *kAppArgsUsage =
-    (GFT_CLI_CC || GFT_CLI_PR) ? "" : "-l: enable thread block load balancer (by default false)";
+    GFT_CLI_NO_SOURCE ? "" : "-l: enable thread block load balancer (by default false)";
 
 static void usage(const char *argv0)
 {
@@ -115,7 +120,8 @@ int main(int argc, char **argv)
     const char *input = argv[optind];
 
     fprintf(stderr, "OPTIONS: gft engine (libgft %d, sm_100a %s)\n", gft_version(),
-            GFT_CLI_PR ? "persistent residual-push PageRank" : GFT_CLI_CC ? "union-find CC"
+            GFT_CLI_MIS  ? "persistent round-based MIS"
+            : GFT_CLI_PR ? "persistent residual-push PageRank" : GFT_CLI_CC ? "union-find CC"
             : GFT_CLI_SSSP ? "persistent near-far SSSP" : "persistent BFS");
     gft_csr h;
     uint64_t t0 = now_ns();
@@ -123,7 +129,7 @@ int main(int argc, char **argv)
     if (s != GFT_OK) return die("read", s);
     printf("nnodes=%u, nedges=%u.\n", h.nnodes, h.nedges);
     printf("read %s in %llu ms\n", input, (unsigned long long)((now_ns() - t0) / 1000000));
-    if (!GFT_CLI_CC && !GFT_CLI_PR && (uint32_t)start_node >= h.nnodes) {
+    if (!GFT_CLI_NO_SOURCE && (uint32_t)start_node >= h.nnodes) {
         fprintf(stderr, "start node %d out of range (%u nodes)\n", start_node, h.nnodes);
         gft_csr_free(&h);
         return EXIT_FAILURE;
@@ -140,7 +146,9 @@ int main(int argc, char **argv)
     uint64_t comps = 0;
     std::vector<float> rank(GFT_CLI_PR ? h.nnodes : 0);
     uint64_t k0 = now_ns();
-    if (GFT_CLI_PR) {
+    if (GFT_CLI_MIS) {
+        s = gft_mis_host(e, g, val.data(), 0, nullptr, nullptr, &st);
+    } else if (GFT_CLI_PR) {
         s = gft_pr_host(e, g, rank.data(), max_iterations, nullptr, nullptr, &st);
     } else if (GFT_CLI_CC) {
         s = gft_cc_host(e, g, val.data(), nullptr, nullptr, &st, &comps);
@@ -151,7 +159,9 @@ int main(int argc, char **argv)
         s = gft_bfs_host(e, g, (uint32_t)start_node, val.data(), nullptr, nullptr, nullptr, &st);
     }
     uint64_t k1 = now_ns();
-    if (s != GFT_OK) return die(GFT_CLI_PR ? "pr" : GFT_CLI_CC ? "cc" : GFT_CLI_SSSP ? "sssp" : "bfs", s);
+    if (s != GFT_OK)
+        return die(GFT_CLI_MIS ? "mis" : GFT_CLI_PR ? "pr" : GFT_CLI_CC ? "cc" : GFT_CLI_SSSP ? "sssp" : "bfs", s);
+    if (GFT_CLI_MIS) printf("Total steps: %u\n", st.levels);
     if (GFT_CLI_PR) printf("PR took %u iterations\n", st.levels);
     if (GFT_CLI_SSSP) printf("iterations: %u\n", st.levels);
     if (GFT_CLI_CC) printf("components: %llu\n", (unsigned long long)comps);
@@ -180,6 +190,8 @@ int main(int argc, char **argv)
             s = GFT_OK;
         } else if (GFT_CLI_PR) {
             s = gft_write_pr_output(output, h.nnodes, rank.data());
+        } else if (GFT_CLI_MIS) {
+            s = gft_write_mis_output(output, h.nnodes, val.data());
         } else if (GFT_CLI_CC) {
             s = gft_write_cc_output(output, &h, val.data());
         } else {

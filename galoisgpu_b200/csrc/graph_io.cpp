@@ -354,4 +354,33 @@ gft_status gft_write_pr_output(const char *path, uint32_t nnodes, const float *h
     return GFT_OK;
 }
 
+gft_status gft_write_mis_output(const char *path, uint32_t nnodes, const int32_t *h_state)
+{
+    if (!path || (nnodes && !h_state)) return fail(GFT_ERR_INVALID_ARG, "gft_write_mis_output: null argument");
+    bool to_stdout = strcmp(path, "-") == 0;
+    FILE *f = to_stdout ? stdout : fopen(path, "w");
+    if (!f) return fail(GFT_ERR_IO, "gft_write_mis_output: cannot open %s: %s", path, strerror(errno));
+    // The set's size, then its member ids in order (apps/mis/support.cu:
+    // 29-37); members are state 1.
+    unsigned count = 0;
+    for (uint32_t i = 0; i < nnodes; i++) count += h_state[i] == 1;
+    std::string s;
+    s.reserve((size_t)count * 9 + 16);
+    char line[32];
+    s.append(line, snprintf(line, sizeof line, "%u\n", count));
+    bool ok = true;
+    for (uint32_t i = 0; i < nnodes && ok; i++) {
+        if (h_state[i] == 1) s.append(line, snprintf(line, sizeof line, "%d\n", (int)i));
+        if (s.size() >= (1u << 24)) {
+            ok = write_all(f, s.data(), s.size());
+            s.clear();
+        }
+    }
+    ok = ok && write_all(f, s.data(), s.size());
+    if (to_stdout) fflush(f);
+    else if (fclose(f) != 0) ok = false;
+    if (!ok) return fail(GFT_ERR_IO, "gft_write_mis_output: write to %s failed", path);
+    return GFT_OK;
+}
+
 }  // extern "C"

@@ -419,6 +419,31 @@ class Engine:
                                  self._tune(tune), _stream_ptr(stream), C.byref(st)))
         return st.as_dict()
 
+    def mis(self, graph: DeviceGraph, out=None, prio_threads: int = 0, tune: Tune | None = None, stream=None) -> dict:
+        """Maximal independent set (apps/mis): ``out`` (int32 device tensor)
+        receives the reference's node_data, 1 = in the set, 2 = excluded.
+        ``prio_threads`` = 0 uses the reference's priority streams on this
+        device (8 CTAs of 256 threads per SM).  ``levels`` = rounds,
+        ``vertices_reached`` = the set's size."""
+        import torch
+
+        dev = torch.device("cuda", graph.device)
+        if out is None:
+            out = torch.empty(graph.nnodes, dtype=torch.int32, device=dev)
+        st = Stats()
+        check(load().gft_mis(self._h, graph.handle, C.c_void_p(out.data_ptr()), prio_threads, self._tune(tune),
+                             _stream_ptr(stream if stream is not None else torch.cuda.current_stream(dev)),
+                             C.byref(st)))
+        return {"out": out, **st.as_dict()}
+
+    def mis_host(self, graph: DeviceGraph, out: np.ndarray, prio_threads: int = 0, tune: Tune | None = None,
+                 stream=None) -> dict:
+        """Maximal independent set into a host int32 array (end to end)."""
+        st = Stats()
+        check(load().gft_mis_host(self._h, graph.handle, C.c_void_p(out.ctypes.data), prio_threads,
+                                  self._tune(tune), _stream_ptr(stream), C.byref(st)))
+        return st.as_dict()
+
     def bfs_host(self, graph: DeviceGraph, start_node: int, out: np.ndarray, parent: np.ndarray | None = None,
                  tune: Tune | None = None, stream=None) -> dict:
         """End-to-end query with host result buffers (int32 / uint32 numpy)."""
@@ -542,6 +567,13 @@ def write_pr_output(path: str | Path, ranks: np.ndarray) -> None:
     check(load().gft_write_pr_output(str(path).encode(), len(r), C.c_void_p(r.ctypes.data)))
 
 
+def write_mis_output(path: str | Path, state: np.ndarray) -> None:
+    """The set as the reference writes it: its size, then one member id per
+    line (apps/mis/support.cu:18-40)."""
+    st = np.ascontiguousarray(state, dtype=np.int32)
+    check(load().gft_write_mis_output(str(path).encode(), len(st), C.c_void_p(st.ctypes.data)))
+
+
 __all__ = [
     "Batch",
     "CSRGraph",
@@ -555,5 +587,6 @@ __all__ = [
     "output",
     "write_cc_output",
     "write_pr_output",
+    "write_mis_output",
     "_lib",
 ]

@@ -428,6 +428,24 @@ GFT_API gft_status gft_pr_host(gft_engine *e, const gft_graph *g, float *h_rank,
  * 95-101).  path "-" writes to stdout. */
 GFT_API gft_status gft_write_pr_output(const char *path, uint32_t nnodes, const float *h_rank);
 
+/* ---------------------------------------------------------------------------
+ * Maximal independent set: replaces apps/mis gg_main (apps/mis/kernel.cu:
+ * 215-231).  d_state (int32, nnodes entries) receives the reference's
+ * node_data: 1 = in the set, 2 = excluded (NON_INDEPENDENT).  Priorities
+ * follow the reference: one xorshift128 stream per thread of a launch of
+ * prio_threads threads (0 = the reference's grid on this device, 8 CTAs of
+ * 256 threads per SM), so the set is the reference's on the same GPU.
+ * stats->levels = rounds ("Total steps"), stats->vertices_reached = the
+ * set's size, stats->edges_scanned = neighbour words read.
+ * ------------------------------------------------------------------------- */
+GFT_API gft_status gft_mis(gft_engine *e, const gft_graph *g, int32_t *d_state, uint32_t prio_threads,
+                           const gft_tuning *tune, void *stream, gft_stats *stats);
+GFT_API gft_status gft_mis_host(gft_engine *e, const gft_graph *g, int32_t *h_state, uint32_t prio_threads,
+                                const gft_tuning *tune, void *stream, gft_stats *stats);
+/* Writes the reference's MIS text (apps/mis/support.cu:18-40): the set's
+ * size, then one member id per line.  path "-" writes to stdout. */
+GFT_API gft_status gft_write_mis_output(const char *path, uint32_t nnodes, const int32_t *h_state);
+
 /* Reach statistics of a result already on the device: V_r (vertices with a
  * finite value) and E_r (sum of their out-degrees, the edges a top-down
  * traversal must scan).  Waits for `stream`. */

@@ -27,6 +27,12 @@
  *                                 :26-47 (init_1), :49-63 (init_2),
  *                                 :127-236 (pop and push), :271-305 (driver),
  *                                 apps/pr/support.cu:47-104 (output)
+ *   - maximal independent set     apps/mis/kernel.cu:9-17 (states, seeds),
+ *                                 :18-41 (per-thread xorshift priorities),
+ *                                 :65-103 (mark local maxima), :104-149
+ *                                 (drop marked vertices and neighbours),
+ *                                 :151-169 (rounds), apps/mis/support.cu:18-40
+ *                                 (output)
  *
  * The reference's BFS and SSSP results are schedule independent: BFS levels
  * are hop distances and SSSP distances are the unique shortest-path lengths
@@ -409,5 +415,104 @@ int orc_write_pr_output(const char *path, uint32_t nnodes, const float *rank)
     FILE *f = fopen(path, "w");
     if (!f) return -1;
     for (int i = 0; i < (int)nnodes; i++) fprintf(f, "%d %f\n", i, (double)rank[i]);
+    return fclose(f) ? -2 : 0;
+}
+
+/* ---------------------------------------------------------------------- */
+/* Maximal independent set (apps/mis).                                     */
+/*                                                                        */
+/* Priorities (apps/mis/kernel.cu:18-41): thread t of a launch of          */
+/* `nthreads` threads runs Marsaglia's xorshift128 from the state          */
+/* (SEED1..SEED4) ^ t and gives its k-th output to vertex t + k*nthreads.   */
+/* The reference launches it with kernel_sizing's grid (skelapp/skel.cu:   */
+/* 37-43): 8 CTAs per SM of 256 threads.                                   */
+/*                                                                        */
+/* Rounds (:151-169): every vertex still on the worklist is MARKED when no */
+/* out-neighbour other than itself that is not NON_INDEPENDENT beats it in */
+/* (priority, id) order (:65-103, unsigned priorities, larger id wins a     */
+/* tie); then every worklist vertex that is MARKED, or has a MARKED         */
+/* out-neighbour, leaves the worklist, and an unmarked one becomes          */
+/* NON_INDEPENDENT (:104-149).  Marking reads only states fixed before the */
+/* round (a vertex marked in the same round is still not NON_INDEPENDENT), */
+/* so the result does not depend on the schedule.  Returns the rounds run;  */
+/* state[v] ends 1 (in the set) or 2 (excluded), 0 only for n == 0.        */
+/* ---------------------------------------------------------------------- */
+#define ORC_MIS_UNMARKED 0
+#define ORC_MIS_MARKED 1
+#define ORC_MIS_NON_INDEPENDENT 2
+
+void orc_mis_priorities(uint32_t nnodes, uint32_t nthreads, uint32_t *prio)
+{
+    for (uint32_t t = 0; t < nthreads && t < nnodes; t++) {
+        uint32_t x = 0x12345678u ^ t, y = 0xabbdef12u ^ t, z = 0xcafe1234u ^ t, w = 0x09832516u ^ t;
+        for (uint64_t v = t; v < nnodes; v += nthreads) {
+            uint32_t tt = x ^ (x << 11);
+            x = y;
+            y = z;
+            z = w;
+            w = w ^ (w >> 19) ^ tt ^ (tt >> 8);
+            prio[v] = w;
+        }
+    }
+}
+
+int64_t orc_mis(uint32_t nnodes, const uint32_t *row_start, const uint32_t *edge_dst, uint32_t nthreads,
+                int32_t *state)
+{
+    uint32_t *prio = (uint32_t *)malloc((size_t)(nnodes ? nnodes : 1) * 4);
+    uint32_t *cur = (uint32_t *)malloc((size_t)(nnodes ? nnodes : 1) * 4);
+    uint32_t *nxt = (uint32_t *)malloc((size_t)(nnodes ? nnodes : 1) * 4);
+    orc_mis_priorities(nnodes, nthreads, prio);
+    for (uint32_t v = 0; v < nnodes; v++) state[v] = ORC_MIS_UNMARKED;
+    size_t ncur = 0;
+    for (uint32_t v = 0; v < nnodes; v++) cur[ncur++] = v;
+    int64_t steps = 0;
+    while (ncur) {
+        /* mark: decisions read states fixed before this pass */
+        for (size_t i = 0; i < ncur; i++) {
+            uint32_t u = cur[i], best = prio[u], best_id = u;
+            for (uint32_t e = row_start[u]; e < row_start[u + 1]; e++) {
+                uint32_t d = edge_dst[e];
+                if (d == u || state[d] == ORC_MIS_NON_INDEPENDENT) continue;
+                if (prio[d] > best || (prio[d] == best && d > best_id)) {
+                    best = prio[d];
+                    best_id = d;
+                }
+            }
+            if (best_id == u) nxt[i] = 1;
+            else nxt[i] = 0;
+        }
+        for (size_t i = 0; i < ncur; i++)
+            if (nxt[i]) state[cur[i]] = ORC_MIS_MARKED;
+        /* drop */
+        size_t nn = 0;
+        for (size_t i = 0; i < ncur; i++) {
+            uint32_t u = cur[i];
+            int drop = state[u] == ORC_MIS_MARKED;
+            for (uint32_t e = row_start[u]; !drop && e < row_start[u + 1]; e++)
+                if (state[edge_dst[e]] == ORC_MIS_MARKED) drop = 1;
+            if (!drop) nxt[nn++] = u;
+            else if (state[u] == ORC_MIS_UNMARKED) state[u] = ORC_MIS_NON_INDEPENDENT;
+        }
+        uint32_t *t = cur;
+        cur = nxt;
+        nxt = t;
+        ncur = nn;
+        steps++;
+    }
+    free(prio); free(cur); free(nxt);
+    return steps;
+}
+
+/* MIS output (apps/mis/support.cu:18-40): the set's size, then its ids. */
+int orc_write_mis_output(const char *path, uint32_t nnodes, const int32_t *state)
+{
+    FILE *f = fopen(path, "w");
+    if (!f) return -1;
+    unsigned count = 0;
+    for (uint32_t i = 0; i < nnodes; i++) count += state[i] == ORC_MIS_MARKED;
+    fprintf(f, "%u\n", count);
+    for (int i = 0; i < (int)nnodes; i++)
+        if (state[i] == ORC_MIS_MARKED) fprintf(f, "%d\n", i);
     return fclose(f) ? -2 : 0;
 }

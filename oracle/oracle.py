@@ -57,6 +57,12 @@ def load():
         lib.orc_pr.argtypes = [C.c_uint32, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.POINTER(C.c_uint64)]
         lib.orc_write_pr_output.restype = C.c_int
         lib.orc_write_pr_output.argtypes = [C.c_char_p, C.c_uint32, C.c_void_p]
+        lib.orc_mis.restype = C.c_int64
+        lib.orc_mis.argtypes = [C.c_uint32, C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p]
+        lib.orc_mis_priorities.restype = None
+        lib.orc_mis_priorities.argtypes = [C.c_uint32, C.c_uint32, C.c_void_p]
+        lib.orc_write_mis_output.restype = C.c_int
+        lib.orc_write_mis_output.argtypes = [C.c_char_p, C.c_uint32, C.c_void_p]
         lib.orc_write_cc_output.restype = C.c_int
         lib.orc_write_cc_output.argtypes = [C.c_char_p, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
         _lib = lib
@@ -177,6 +183,48 @@ def canonical_labels(label) -> np.ndarray:
     first = np.full(max(n, int(lab.max()) + 1 if n else 0), n, dtype=np.int64)
     np.minimum.at(first, lab, np.arange(n, dtype=np.int64))
     return first[lab].astype(np.int32)
+
+
+# The reference's MIS priority streams on a B200: kernel_sizing launches 8
+# CTAs of 256 threads per SM (skelapp/skel.cu:37-43), 148 SMs.
+MIS_THREADS_B200 = 8 * 148 * 256
+
+
+def mis_priorities(nnodes: int, nthreads: int = MIS_THREADS_B200) -> np.ndarray:
+    """apps/mis/kernel.cu:18-41: per-thread xorshift128 priorities."""
+    out = np.empty(max(nnodes, 1), dtype=np.uint32)[:nnodes]
+    load().orc_mis_priorities(nnodes, nthreads, _p(out))
+    return out
+
+
+def mis(row_start, edge_dst, nthreads: int = MIS_THREADS_B200) -> tuple[np.ndarray, int]:
+    """Maximal independent set by the reference's rounds: (int32 state per
+    vertex, 1 = in the set, 2 = excluded; rounds run)."""
+    rs = np.ascontiguousarray(row_start, dtype=np.uint32)
+    dst = np.ascontiguousarray(edge_dst, dtype=np.uint32)
+    n = len(rs) - 1
+    state = np.empty(max(n, 1), dtype=np.int32)[:n]
+    steps = load().orc_mis(n, _p(rs), _p(dst), nthreads, _p(state))
+    return state, int(steps)
+
+
+def write_mis_output(path, state) -> None:
+    st = np.ascontiguousarray(state, dtype=np.int32)
+    if load().orc_write_mis_output(str(path).encode(), len(st), _p(st)) != 0:
+        raise OSError(f"cannot write {path}")
+
+
+def read_mis_output(path, nnodes: int) -> np.ndarray:
+    """Parses the reference's MIS text (count, then member ids) into a
+    membership mask; checks the count line."""
+    lines = Path(path).read_text().split()
+    count = int(lines[0])
+    ids = np.array([int(x) for x in lines[1:]], dtype=np.int64)
+    if len(ids) != count:
+        raise ValueError(f"{path}: count line says {count}, {len(ids)} ids follow")
+    mask = np.zeros(nnodes, dtype=bool)
+    mask[ids] = True
+    return mask
 
 
 def pr(row_start, edge_dst, max_iterations: int = 2**62, stats: dict | None = None) -> tuple[np.ndarray, int]:

@@ -102,7 +102,7 @@ def test_cli_binaries_are_the_right_apps():
     if not (b.BIN / "bfs").exists():
         b.build()
     for app, has_delta, has_src in (("bfs", False, True), ("sssp", True, True), ("cc", False, False),
-                                    ("pr", False, False)):
+                                    ("pr", False, False), ("mis", False, False)):
         r = subprocess.run([str(b.BIN / app)], capture_output=True, text=True, timeout=60)
         assert r.returncode != 0
         assert "usage:" in r.stderr and ("[-s startNode]" in r.stderr) == has_src, r.stderr
