@@ -26,9 +26,9 @@ one JSON line.
   secondary    N = 1 only: BFS on RMAT-24 (64 seeded sources, harmonic-mean
                GTEPS) and on the 256^2 grid; 512 batched SSSP queries;
                256-source BFS on RMAT-24; serving 8 resident graphs under
-               Poisson load; connected components and PageRank on RMAT-24
-               and the road grid (--workload cc-rmat-24, pr-road-4096, ...
-               runs one alone)
+               Poisson load; connected components, PageRank and maximal
+               independent set on RMAT-24 and the road grid (--workload
+               cc-rmat-24, pr-road-4096, mis-rmat-24, ... runs one alone)
 
 --impl reference runs the reference arm: the reference has no CPU
 implementation of this path, so the oracle's restatement of it (kind
@@ -469,6 +469,12 @@ def our_arm(args) -> int:
                 sec["serve-8-graphs"] = bench_serve(gft, dev)
             except Exception as ex:
                 sec["serve-8-graphs"] = {"error": repr(ex)}
+            for mname in MIS_WORKLOADS:
+                try:
+                    torch.cuda.empty_cache()
+                    sec[mname] = bench_mis(gft, orc, mname, dev)
+                except Exception as ex:
+                    sec[mname] = {"error": repr(ex)}
             for pname in PR_SECONDARY:
                 try:
                     torch.cuda.empty_cache()
@@ -550,6 +556,77 @@ def bench_cc(gft, orc, name: str, dev: int, steps: int = 10, warmup: int = 3) ->
     }
     log(f"[{name}] {res['value']:.1f} GTEPS, kernel {kernel_ms:.3f} ms, {r['components']} components, "
         f"parity {res['parity_vs_oracle']}")
+    eng.close()
+    dg.free()
+    return res
+
+
+MIS_WORKLOADS = {
+    "mis-rmat-24": dict(kind="rmat", scale=24, edge_factor=16, seed=1),
+    "mis-road-4096": dict(kind="road", side=4096, seed=1),
+}
+
+
+def bench_mis(gft, orc, name: str, dev: int, steps: int = 10, warmup: int = 3) -> dict:
+    """Maximal independent set (apps/mis on this engine) on a full-size seeded
+    graph with the reference's priorities on this device: GTEPS = all E
+    directed edges / kernel time, end to end with the states copied to
+    pinned host memory, the oracle's rounds on one host core as CPU
+    baseline, and bit-exact parity of the set and the round count."""
+    import torch
+
+    spec = {**MIS_WORKLOADS[name], "app": "mis"}
+    dg = make_device_graph(gft, spec, dev)
+    host = dg.download()
+    eng = gft.Engine(dev)
+    out = torch.empty(dg.nnodes, dtype=torch.int32, device=f"cuda:{dev}")
+    stream = torch.cuda.current_stream(dev)
+    for _ in range(warmup):
+        r = eng.mis(dg, out=out, stream=stream)
+    torch.cuda.synchronize(dev)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    kms = []
+    for _ in range(steps):
+        r = eng.mis(dg, out=out, stream=stream)
+        kms.append(r["kernel_ms"])
+    ev1.record(stream)
+    torch.cuda.synchronize(dev)
+    total_ms = ev0.elapsed_time(ev1)
+    kernel_ms = statistics.mean(kms)
+    h_out = torch.empty(dg.nnodes, dtype=torch.int32, pin_memory=True).numpy()
+    eng.mis_host(dg, h_out)
+    t1 = time.perf_counter()
+    for _ in range(steps):
+        eng.mis_host(dg, h_out)
+    e2e_s = (time.perf_counter() - t1) / steps
+    prio_threads = 8 * torch.cuda.get_device_properties(dev).multi_processor_count * 256
+    t2 = time.perf_counter()
+    want, want_steps = orc.mis(host.row_start, host.edge_dst, prio_threads)
+    cpu_s = time.perf_counter() - t2
+    peak, peak_kind = measured_peaks()
+    # Bytes the rounds must move: per neighbour tested its id and packed
+    # word (12 B); per worklist entry and pass the entry, the vertex's own
+    # word and its row pair (20 B, two passes); per vertex the priority
+    # word and worklist entry written at the start and the word read and
+    # state written at the end (24 B).
+    alg = 12 * r["edges_scanned"] + 40 * r["pushes"] + 24 * dg.nnodes
+    res = {
+        "metric": "GTEPS (all edges)", "value": dg.nedges / (total_ms / steps * 1e6), "unit": "GTEPS",
+        "kernel_ms_mean": kernel_ms, "steps": steps, "warmup": warmup, "nodes": dg.nnodes, "edges": dg.nedges,
+        "rounds": r["levels"], "set_size": r["vertices_reached"], "neighbours_tested": r["edges_scanned"],
+        "worklist_entries": r["pushes"], "prio_threads": prio_threads,
+        "e2e": {"value": dg.nedges / (e2e_s * 1e9), "unit": "GTEPS", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": dg.nnodes * 4},
+        "roofline": {"bound": "hbm", "achieved": alg / (kernel_ms * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
+                     "frac": alg / (kernel_ms * 1e-3) / 1e9 / peak, "traffic": None, "peak_kind": peak_kind,
+                     "alg_bytes_per_launch": alg, "kernel": "mis_persistent"},
+        "cpu_baseline": {"value": dg.nedges / cpu_s / 1e9, "unit": "GTEPS", "cores": 1, "kind": "port",
+                         "sample": f"the oracle's full MIS ({want_steps} rounds, {cpu_s:.1f} s)"},
+        "parity_vs_oracle": "bit-exact" if np.array_equal(h_out, want) and want_steps == r["levels"] else "MISMATCH",
+    }
+    log(f"[{name}] {res['value']:.1f} GTEPS, kernel {kernel_ms:.3f} ms, {r['levels']} rounds, "
+        f"set {r['vertices_reached']}, parity {res['parity_vs_oracle']}")
     eng.close()
     dg.free()
     return res
@@ -931,35 +1008,37 @@ def main(argv=None) -> int:
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("gft", "reference"), default="gft")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS) + sorted(CC_WORKLOADS) + sorted(PR_WORKLOADS),
-                    default=HEADLINE, help="a traversal workload (the headline by default), or a connected-components "
-                                           "or PageRank one")
+    ap.add_argument("--workload",
+                    choices=sorted(WORKLOADS) + sorted(CC_WORKLOADS) + sorted(PR_WORKLOADS) + sorted(MIS_WORKLOADS),
+                    default=HEADLINE, help="a traversal workload (the headline by default), or a connected-components, "
+                                           "PageRank or maximal-independent-set one")
     ap.add_argument("--no-secondary", action="store_true", help="skip the secondary workloads")
     args = ap.parse_args(argv)
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
     if args.impl == "reference":
         return reference_arm(args)
-    if args.workload in CC_WORKLOADS or args.workload in PR_WORKLOADS:
+    if args.workload in CC_WORKLOADS or args.workload in PR_WORKLOADS or args.workload in MIS_WORKLOADS:
         return cc_arm(args)
     return our_arm(args)
 
 
 def cc_arm(args) -> int:
-    """One connected-components or PageRank workload on one GPU, as a JSON
-    line."""
+    """One connected-components, PageRank or maximal-independent-set
+    workload on one GPU, as a JSON line."""
     import torch
 
     import galoisgpu_b200 as gft
     from oracle import oracle as orc
 
     torch.cuda.set_device(0)
-    is_pr = args.workload in PR_WORKLOADS
-    r = (bench_pr if is_pr else bench_cc)(gft, orc, args.workload, 0, steps=args.steps, warmup=args.warmup)
+    is_pr, is_mis = args.workload in PR_WORKLOADS, args.workload in MIS_WORKLOADS
+    fn, table = (bench_pr, PR_WORKLOADS) if is_pr else (bench_mis, MIS_WORKLOADS) if is_mis else (bench_cc, CC_WORKLOADS)
+    r = fn(gft, orc, args.workload, 0, steps=args.steps, warmup=args.warmup)
     line = {**r, "n_gpus": 1, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32" if is_pr else "u32",
             "data": "synthetic: seeded graph generated on the device (SplitMix64 streams)",
-            "config": {"workload": args.workload, **(PR_WORKLOADS if is_pr else CC_WORKLOADS)[args.workload]}}
+            "config": {"workload": args.workload, **table[args.workload]}}
     print(json.dumps(line), flush=True)
     return 0
 

@@ -169,12 +169,13 @@ __device__ __forceinline__ void mis_body(const MisParams &mp, Mode &m, uint32_t 
     q.cap = p.qcap;
     q.err = &ctl->error;
     q.err_where = &ctl->error_where;
-    unsigned long long scanned = 0;
+    unsigned long long scanned = 0, pops = 0;  // pops: thread 0's tally of worklist entries
     unsigned L = 0;
     for (;;) {
         const unsigned slot = L % 3, nslot = (L + 1) % 3, rslot = (L + 2) % 3;
         const unsigned n_in = m.ld(u32_of(ctl->qlen[slot]));
         if (n_in == 0) break;
+        pops += n_in;
         if (tid == 0) {
             *u32_of(ctl->qlen[rslot]) = 0;
             *u32_of(ctl->claim[rslot]) = 0;
@@ -201,6 +202,7 @@ __device__ __forceinline__ void mis_body(const MisParams &mp, Mode &m, uint32_t 
     if (tid == 0) {
         ctl->levels = L;
         ctl->iterations = m.epoch();
+        ctl->pushes = pops;
     }
 }
 
@@ -237,6 +239,7 @@ __global__ void __launch_bounds__(kMisBlock, 1) mis_single_cta(MisParams mp)
         gctl->iterations = s_ctl.iterations;
         gctl->edges = s_ctl.edges;
         gctl->reached = s_ctl.reached;
+        gctl->pushes = s_ctl.pushes;
     }
 }
 
@@ -341,6 +344,7 @@ gft_status run_mis(gft_engine *e, const gft_graph *g, int32_t *d_state, uint32_t
         stats->iterations = h->iterations;
         stats->vertices_reached = h->reached;
         stats->edges_scanned = h->edges;
+        stats->pushes = h->pushes;
         stats->kernel_ms = ms;
         stats->grid_blocks = shape.blocks;
         stats->block_threads = shape.block_threads;

@@ -436,7 +436,8 @@ GFT_API gft_status gft_write_pr_output(const char *path, uint32_t nnodes, const 
  * prio_threads threads (0 = the reference's grid on this device, 8 CTAs of
  * 256 threads per SM), so the set is the reference's on the same GPU.
  * stats->levels = rounds ("Total steps"), stats->vertices_reached = the
- * set's size, stats->edges_scanned = neighbour words read.
+ * set's size, stats->edges_scanned = neighbour words read, stats->pushes =
+ * worklist entries over all rounds.
  * ------------------------------------------------------------------------- */
 GFT_API gft_status gft_mis(gft_engine *e, const gft_graph *g, int32_t *d_state, uint32_t prio_threads,
                            const gft_tuning *tune, void *stream, gft_stats *stats);

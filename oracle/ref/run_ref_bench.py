@@ -1,15 +1,16 @@
 """Times the reference's own CUDA build (oracle/_ref, built by
 oracle/ref/Makefile from the reference sources) on the full-size seeded
 configurations, the way a user runs it: ``bfs|sssp -q -s <src> [-d delta]
-<graph.gr>``, ``cc -q <graph.gr>`` or ``pr -q <graph.gr>``, one process per
-query, reading its
+<graph.gr>``, ``cc -q <graph.gr>``, ``pr -q <graph.gr>`` or ``mis -q
+<graph.gr>``, one process per query, reading its
 ``Total time: N ns`` line
 (reference skelapp/skel.cu:159-166; that time includes the worklist
 allocations gg_main makes, apps/bfs/kernel.cu:389, apps/sssp/kernel.cu:475).
 Kernel-only time comes from running this same script under
 ``ncu --metrics gpu__time_duration.sum -k regex:gg_main_pipe`` (for cc, every
 kernel of the process: its driver is a host loop of launches; for pr the
-init kernels and the persistent gg_main_pipe_1_gpu_gb).
+init kernels and the persistent gg_main_pipe_1_gpu_gb; for mis gen_prio_gpu
+and the round kernels).
 
 Test/measurement infrastructure only: the input graphs are produced with this
 repository's generator, and E_r comes from this repository's engine (whose
@@ -50,7 +51,41 @@ CONFIGS = {
     "cc-road4096": dict(kind="road", kw=dict(side=4096), seed=1, app="cc", src_seed=None),
     "pr-rmat24": dict(kind="rmat", kw=dict(scale=24, edge_factor=16), seed=1, app="pr", src_seed=None),
     "pr-road4096": dict(kind="road", kw=dict(side=4096), seed=1, app="pr", src_seed=None),
+    "mis-rmat24": dict(kind="rmat", kw=dict(scale=24, edge_factor=16), seed=1, app="mis", src_seed=None),
+    "mis-road4096": dict(kind="road", kw=dict(side=4096), seed=1, app="mis", src_seed=None),
 }
+
+
+def run_mis(a, c, dg, host, eng, gr: Path) -> int:
+    """The reference's MIS (oracle/_ref/mis: its kernels through its host
+    round loop) against this engine's: total time, rounds, and with --check
+    whether the sets are identical."""
+    mine = eng.mis(dg)
+    cmd = [str(REF / "mis")]
+    out = Path(a.workdir) / f"gft_{a.config}.mis.out"
+    cmd += ["-o", str(out)] if a.check else ["-q"]
+    t = time.time()
+    r = subprocess.run(cmd + [str(gr)], capture_output=True, text=True, timeout=1800)
+    wall = time.time() - t
+    if r.returncode != 0:
+        print(r.stdout, r.stderr, file=sys.stderr)
+        return r.returncode
+    m = re.search(r"Total time: (\d+) ns", r.stderr)
+    ns = int(m.group(1)) if m else None
+    steps = int(re.search(r"Total steps: (\d+)", r.stdout).group(1))
+    rec = {"config": a.config, "app": "mis", "total_time_ns": ns, "steps": steps, "edges": dg.nedges,
+           "gft_kernel_ms": mine["kernel_ms"], "gft_steps": mine["levels"], "gft_set_size": mine["vertices_reached"],
+           "process_wall_s": wall}
+    ok = steps == mine["levels"]
+    if a.check:
+        ref = orc.read_mis_output(out, host.nnodes)
+        same = bool(np.array_equal(ref, mine["out"].cpu().numpy() == 1))
+        rec["parity_vs_gft"] = "identical set" if same else "MISMATCH"
+        ok = ok and same
+        out.unlink()
+    print(json.dumps(rec), flush=True)
+    gr.unlink()
+    return 0 if ok else 1
 
 
 def run_pr(a, c, dg, host, eng, gr: Path) -> int:
@@ -108,6 +143,8 @@ def main(argv=None) -> int:
     results = []
     if c["app"] == "pr":
         return run_pr(a, c, dg, host, eng, gr)
+    if c["app"] == "mis":
+        return run_mis(a, c, dg, host, eng, gr)
     if c["app"] == "cc":
         # Component count only: the reference's CC output lists every edge
         # (apps/cc/support.cu:30-35), about 15 GB of text for RMAT-24.
