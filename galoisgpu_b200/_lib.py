@@ -76,6 +76,7 @@ class Tuning(C.Structure):
         ("group_blocks", C.c_uint32),
         ("group_min_nodes", C.c_uint32),
         ("direction", C.c_uint32),
+        ("cta_small", C.c_uint32),
     ]
 
 

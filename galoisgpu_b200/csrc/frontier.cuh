@@ -51,6 +51,7 @@ struct TravParams {
     uint32_t nedges;
     int dir_opt;  // BFS: direction-optimising (graph marked symmetric)
     int uniform;  // every out-degree <= kUniformDegree: static chunks
+    uint32_t cta_small;  // SSSP on the grid: iterations of at most this many vertices run on one CTA (0 = never)
 };
 
 // ---------------------------------------------------------------------------
@@ -499,6 +500,7 @@ __device__ __forceinline__ void bottom_up_level(BfsVisitor &vis, const TravParam
 // against this interface.
 // ---------------------------------------------------------------------------
 struct GridMode {
+    static constexpr bool kGrid = true;
     GridSync gs;
     TraversalCtl *ctl;
     unsigned tid, nthreads, gwarp, nwarps;
@@ -509,7 +511,8 @@ struct GridMode {
 };
 
 struct CtaMode {
-    TraversalCtl *ctl;  // in shared memory
+    static constexpr bool kGrid = false;
+    TraversalCtl *ctl;  // in shared memory, or the grid's control block while one CTA runs alone
     unsigned tid, nthreads, gwarp, nwarps, ep;
     // Every thread contributes its own view of the error word, so all threads
     // take the same decision even if an error is raised as the barrier opens.
@@ -666,6 +669,126 @@ __device__ __forceinline__ void bfs_body(const TravParams &p, Mode &m, uint32_t 
 // ---------------------------------------------------------------------------
 // SSSP body (near-far)
 // ---------------------------------------------------------------------------
+// Near-far loop state: bucket threshold (inclusive), iteration, phase.
+struct SsspState {
+    unsigned long long T;
+    unsigned I, P;
+};
+
+// Is the coming iteration small enough for one CTA?  A near pile of at most
+// p.cta_small vertices, or a far split (empty near pile) of a far pile that
+// small.
+template <class Mode>
+__device__ __forceinline__ bool sssp_small(const TravParams &p, Mode &m, const SsspState &st, unsigned n_near)
+{
+    if (n_near) return n_near <= p.cta_small;
+    return m.ld(u32_of(m.ctl->far_len[st.P % 3])) <= p.cta_small;
+}
+
+// One near-far iteration (apps/sssp/kernel.cu:177-306 for the relaxation):
+// relax the near pile, or, when it is empty, split the far pile with the
+// next threshold.  gwarp/nwarps are the caller's warp numbering for the
+// work split (the grid's, or one CTA's).  Returns 0 to go on, 1 when the
+// traversal is done (both piles empty), -1 when a barrier reported an error.
+template <class Mode>
+__device__ __forceinline__ int sssp_iter(const TravParams &p, Mode &m, SsspVisitor &vis, SsspState &st,
+                                         unsigned n_near, unsigned gwarp, unsigned nwarps)
+{
+    TraversalCtl *ctl = m.ctl;
+    const unsigned lane = threadIdx.x & 31;
+    const unsigned tid = m.tid;
+    const unsigned I = st.I, P = st.P;
+    const unsigned long long T = st.T;
+    const unsigned slot = I % 3, nslot = (I + 1) % 3, rslot = (I + 2) % 3;
+    if (tid == 0) {
+        trace_iter(I, n_near | ((unsigned long long)m.ld(u32_of(ctl->far_len[P % 3])) << 32));
+        *u32_of(ctl->qlen[rslot]) = 0;
+        *u32_of(ctl->claim[rslot]) = 0;
+        ctl->hub[rslot].v = 0;
+        *u32_of(ctl->hub_claim[rslot]) = 0;
+    }
+    vis.nq.queue = sel2(p.q, (I + 1));
+    vis.nq.len = u32_of(ctl->qlen[nslot]);
+    if (n_near > 0) {
+        // Relax the near pile (apps/sssp/kernel.cu:177-306).
+        vis.threshold = T;
+        vis.near_tag = 2 * I + 3;  // odd, distinct per iteration, never the initial 0
+        vis.far_tag = P + 1;
+        vis.far_min = kInf;
+        vis.fq.queue = sel2(p.far, P);
+        vis.fq.len = u32_of(ctl->far_len[P % 3]);
+        expand_frontier<SsspVisitor, SsspOwn>(vis, p, sel2(p.q, I), n_near, u32_of(ctl->claim[slot]),
+                                              &ctl->hub[slot].v, pick_grain(n_near, nwarps, p.uniform), gwarp, nwarps,
+                                              lane);
+        vis.nq.flush(lane);
+        vis.fq.flush(lane);
+        unsigned fm = warp_min_u32(vis.far_min);
+        if (lane == 0 && fm != kInf) atomicMin(u32_of(ctl->far_min[P % 3]), fm);
+        if (!m.sync()) return -1;
+        const unsigned long long hv = m.ld64(&ctl->hub[slot].v);
+        if (hv) {
+            vis.far_min = kInf;
+            expand_hubs<SsspVisitor, SsspOwn>(vis, p, (unsigned)(hv >> 32), (unsigned)hv,
+                                              u32_of(ctl->hub_claim[slot]), gwarp, nwarps, lane);
+            vis.nq.flush(lane);
+            vis.fq.flush(lane);
+            fm = warp_min_u32(vis.far_min);
+            if (lane == 0 && fm != kInf) atomicMin(u32_of(ctl->far_min[P % 3]), fm);
+            if (!m.sync()) return -1;
+        }
+    } else {
+        // Near pile drained: split the far pile with the next threshold.
+        const unsigned nf = m.ld(u32_of(ctl->far_len[P % 3]));
+        if (nf == 0) return 1;
+        const unsigned fmin = m.ld(u32_of(ctl->far_min[P % 3]));
+        const unsigned long long T_old = T;
+        unsigned long long T_new = T_old + p.delta;
+        if (fmin != kInf && fmin > T_new)  // skip empty buckets
+            T_new = T_old + (unsigned long long)p.delta * ((fmin - T_old + p.delta - 1) / p.delta);
+        if (tid == 0) {
+            *u32_of(ctl->far_len[(P + 2) % 3]) = 0;
+            *u32_of(ctl->far_min[(P + 2) % 3]) = kInf;
+        }
+        vis.fq.queue = sel2(p.far, (P + 1));
+        vis.fq.len = u32_of(ctl->far_len[(P + 1) % 3]);
+        const uint32_t *pile = sel2(p.far, P);
+        unsigned local_min = kInf;
+        const unsigned sgrain = pick_grain(nf, nwarps, p.uniform);
+        const ChunkSched cs{(nf + sgrain - 1) / sgrain, nwarps, gwarp, lane, u32_of(ctl->claim[slot])};
+        for (unsigned c = cs.first(); c < cs.nchunks; c = cs.next()) {
+            const unsigned base = c * sgrain;
+            const unsigned end = min(nf, base + sgrain);
+            for (unsigned i0 = base; i0 < end; i0 += 32) {
+                const unsigned idx = i0 + lane;
+                uint32_t v = 0;
+                unsigned d = kInf;
+                if (idx < end) {
+                    v = __ldcg(pile + idx);
+                    d = (uint32_t)(__ldcg(p.dt + v) >> 32);
+                }
+                const bool live = idx < end && d > T_old;
+                const bool to_near = live && d <= T_new;
+                const bool to_far = live && d > T_new;
+                if (to_far) {
+                    p.far_stamp[v] = P + 2;
+                    local_min = min(local_min, d);
+                }
+                vis.nq.push(to_near, v, lane);
+                vis.fq.push(to_far, v, lane);
+            }
+        }
+        vis.nq.flush(lane);
+        vis.fq.flush(lane);
+        unsigned fm = warp_min_u32(local_min);
+        if (lane == 0 && fm != kInf) atomicMin(u32_of(ctl->far_min[(P + 1) % 3]), fm);
+        if (!m.sync()) return -1;
+        st.T = T_new;
+        st.P = P + 1;
+    }
+    st.I = I + 1;
+    return 0;
+}
+
 template <class Mode>
 __device__ __forceinline__ void sssp_body(const TravParams &p, Mode &m, uint32_t *near_buf, uint32_t *far_buf)
 {
@@ -704,97 +827,41 @@ __device__ __forceinline__ void sssp_body(const TravParams &p, Mode &m, uint32_t
     vis.fq = vis.nq;
     vis.fq.buf = far_buf;
 
-    unsigned long long T = p.delta;  // current bucket threshold (inclusive)
-    unsigned I = 0, P = 0;           // iteration, phase
+    SsspState st{p.delta, 0, 0};
     for (;;) {
-        const unsigned slot = I % 3, nslot = (I + 1) % 3, rslot = (I + 2) % 3;
-        const unsigned n_near = m.ld(u32_of(ctl->qlen[slot]));
-        if (tid == 0) {
-            trace_iter(I, n_near | ((unsigned long long)m.ld(u32_of(ctl->far_len[P % 3])) << 32));
-            *u32_of(ctl->qlen[rslot]) = 0;
-            *u32_of(ctl->claim[rslot]) = 0;
-            ctl->hub[rslot].v = 0;
-            *u32_of(ctl->hub_claim[rslot]) = 0;
-        }
-        vis.nq.queue = sel2(p.q, (I + 1));
-        vis.nq.len = u32_of(ctl->qlen[nslot]);
-        if (n_near > 0) {
-            // Relax the near pile (apps/sssp/kernel.cu:177-306).
-            vis.threshold = T;
-            vis.near_tag = 2 * I + 3;  // odd, distinct per iteration, never the initial 0
-            vis.far_tag = P + 1;
-            vis.far_min = kInf;
-            vis.fq.queue = sel2(p.far, P);
-            vis.fq.len = u32_of(ctl->far_len[P % 3]);
-            expand_frontier<SsspVisitor, SsspOwn>(vis, p, sel2(p.q, I), n_near, u32_of(ctl->claim[slot]),
-                                                  &ctl->hub[slot].v, pick_grain(n_near, nwarps, p.uniform), gwarp, nwarps, lane);
-            vis.nq.flush(lane);
-            vis.fq.flush(lane);
-            unsigned fm = warp_min_u32(vis.far_min);
-            if (lane == 0 && fm != kInf) atomicMin(u32_of(ctl->far_min[P % 3]), fm);
-            if (!m.sync()) return;
-            const unsigned long long hv = m.ld64(&ctl->hub[slot].v);
-            if (hv) {
-                vis.far_min = kInf;
-                expand_hubs<SsspVisitor, SsspOwn>(vis, p, (unsigned)(hv >> 32), (unsigned)hv,
-                                                  u32_of(ctl->hub_claim[slot]), gwarp, nwarps, lane);
-                vis.nq.flush(lane);
-                vis.fq.flush(lane);
-                fm = warp_min_u32(vis.far_min);
-                if (lane == 0 && fm != kInf) atomicMin(u32_of(ctl->far_min[P % 3]), fm);
-                if (!m.sync()) return;
-            }
-        } else {
-            // Near pile drained: split the far pile with the next threshold.
-            const unsigned nf = m.ld(u32_of(ctl->far_len[P % 3]));
-            if (nf == 0) break;
-            const unsigned fmin = m.ld(u32_of(ctl->far_min[P % 3]));
-            const unsigned long long T_old = T;
-            unsigned long long T_new = T_old + p.delta;
-            if (fmin != kInf && fmin > T_new)  // skip empty buckets
-                T_new = T_old + (unsigned long long)p.delta * ((fmin - T_old + p.delta - 1) / p.delta);
-            if (tid == 0) {
-                *u32_of(ctl->far_len[(P + 2) % 3]) = 0;
-                *u32_of(ctl->far_min[(P + 2) % 3]) = kInf;
-            }
-            vis.fq.queue = sel2(p.far, (P + 1));
-            vis.fq.len = u32_of(ctl->far_len[(P + 1) % 3]);
-            const uint32_t *pile = sel2(p.far, P);
-            unsigned local_min = kInf;
-            const unsigned sgrain = pick_grain(nf, nwarps, p.uniform);
-            const ChunkSched cs{(nf + sgrain - 1) / sgrain, nwarps, gwarp, lane, u32_of(ctl->claim[slot])};
-            for (unsigned c = cs.first(); c < cs.nchunks; c = cs.next()) {
-                const unsigned base = c * sgrain;
-                const unsigned end = min(nf, base + sgrain);
-                for (unsigned i0 = base; i0 < end; i0 += 32) {
-                    const unsigned idx = i0 + lane;
-                    uint32_t v = 0;
-                    unsigned d = kInf;
-                    if (idx < end) {
-                        v = __ldcg(pile + idx);
-                        d = (uint32_t)(__ldcg(dt + v) >> 32);
-                    }
-                    const bool live = idx < end && d > T_old;
-                    const bool to_near = live && d <= T_new;
-                    const bool to_far = live && d > T_new;
-                    if (to_far) {
-                        p.far_stamp[v] = P + 2;
-                        local_min = min(local_min, d);
-                    }
-                    vis.nq.push(to_near, v, lane);
-                    vis.fq.push(to_far, v, lane);
+        const unsigned n_near = m.ld(u32_of(ctl->qlen[st.I % 3]));
+        if (Mode::kGrid && p.cta_small && sssp_small(p, m, st, n_near)) {
+            // Small iterations: the first CTA runs them alone, with
+            // __syncthreads as the barrier, while the other CTAs wait at the
+            // grid barrier below; it hands the loop state over there.
+            if (blockIdx.x == 0) {
+                CtaMode cm{ctl, threadIdx.x, blockDim.x, threadIdx.x >> 5, blockDim.x >> 5, 0};
+                unsigned nn = n_near;
+                int r = 0;
+                do {
+                    r = sssp_iter(p, cm, vis, st, nn, threadIdx.x >> 5, blockDim.x >> 5);
+                    if (r != 0) break;
+                    nn = cm.ld(u32_of(ctl->qlen[st.I % 3]));
+                } while (sssp_small(p, cm, st, nn));
+                if (threadIdx.x == 0) {
+                    ctl->handoff[0].v = st.T;
+                    ctl->handoff[1].v = ((unsigned long long)(r > 0) << 63) | ((unsigned long long)st.P << 32) | st.I;
                 }
             }
-            vis.nq.flush(lane);
-            vis.fq.flush(lane);
-            unsigned fm = warp_min_u32(local_min);
-            if (lane == 0 && fm != kInf) atomicMin(u32_of(ctl->far_min[(P + 1) % 3]), fm);
             if (!m.sync()) return;
-            T = T_new;
-            P++;
+            const unsigned long long h1 = m.ld64(&ctl->handoff[1].v);
+            st.T = m.ld64(&ctl->handoff[0].v);
+            st.I = (unsigned)h1;
+            st.P = (unsigned)(h1 >> 32) & 0x7FFFFFFFu;
+            if (h1 >> 63) break;
+            continue;
         }
-        I++;
+        const int r = sssp_iter(p, m, vis, st, n_near, gwarp, nwarps);
+        if (r < 0) return;
+        if (r > 0) break;
     }
+    const unsigned long long T = st.T;
+    const unsigned P = st.P;
     // Every CTA leaves the loop after the same barrier, so all relaxations are
     // done: write the int32 distances.
     for (uint32_t v = tid; v < n; v += nthreads) p.out[v] = (int32_t)(uint32_t)(__ldcg(dt + v) >> 32);

@@ -75,6 +75,8 @@ struct TraversalCtl {
     CtlLine far_len[3];    // SSSP far pile length per phase slot (u32)
     CtlLine far_min[3];    // SSSP least distance sent to the far pile per phase slot (u32)
     CtlLine job;           // batch kernel: job claimed by a CTA group (u32)
+    CtlLine handoff[2];    // SSSP: loop state left by the CTA that ran small iterations alone
+                           // ([0] threshold; [1] done << 63 | phase << 32 | iteration)
     // Cold fields, written once per launch.
     unsigned error;        // gft_status recorded by the device (0 = none)
     unsigned error_where;  // barrier episode or queue index of the failure

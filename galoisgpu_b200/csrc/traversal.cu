@@ -168,6 +168,12 @@ constexpr uint32_t kDefaultBlockSssp = 512;
 constexpr uint32_t kDefaultBlocksPerSm = 2;
 constexpr uint32_t kDefaultHubDegree = 256;
 constexpr uint32_t kDefaultTimeoutMs = 20000;
+// SSSP iterations of at most this many vertices (near pile, or far pile at a
+// split) run on the grid's first CTA alone, by default on graphs of uniform
+// degree: a __syncthreads saves the grid barrier, but one CTA's warps take
+// longer over the pile, so only tiny piles gain (road 4096^2: 4.81 ->
+// 4.73 ms at 256, slower from 1024 up; R-MAT gains nothing).
+constexpr uint32_t kDefaultCtaSmall = 256;
 // Graphs up to this size run on one CTA by default: their frontiers are
 // small enough for 1024 threads, and a __syncthreads per level is several
 // times cheaper than a grid barrier (BFS on the 256^2 grid: 511 levels).
@@ -199,12 +205,13 @@ struct Tune {
     int skip;
     uint32_t max_blocks;
     uint32_t direction;
+    uint32_t cta_small;
 };
 
 Tune resolve_tuning(const gft_tuning *t, bool is_sssp)
 {
     Tune r{is_sssp ? kDefaultBlockSssp : kDefaultBlockBfs, kDefaultBlocksPerSm, kDefaultHubDegree, kDefaultTimeoutMs,
-           -1, 0, 0};
+           -1, 0, 0, 0};
     if (t) {
         if (t->block_threads) r.block = t->block_threads;
         if (t->blocks_per_sm) r.bps = t->blocks_per_sm;
@@ -213,6 +220,7 @@ Tune resolve_tuning(const gft_tuning *t, bool is_sssp)
         r.skip = t->test_skip_block;
         r.max_blocks = t->max_blocks;
         r.direction = t->direction;
+        r.cta_small = t->cta_small;
     }
     return r;
 }
@@ -331,6 +339,8 @@ gft_status run_traversal(bool is_sssp, gft_engine *e, const gft_graph *g, uint32
     p.nedges = G.nedges;
     p.dir_opt = !is_sssp && G.symmetric && t.direction == 0;
     p.uniform = G.max_degree <= kUniformDegree;
+    if (is_sssp && !single)
+        p.cta_small = t.cta_small == UINT32_MAX ? 0 : t.cta_small ? t.cta_small : p.uniform ? kDefaultCtaSmall : 0;
 
     GFT_CUDA_TRY(cudaMemsetAsync(e->ctl.ptr, 0, sizeof(TraversalCtl), stream));
     void *args[] = {&p};

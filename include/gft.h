@@ -96,6 +96,11 @@ typedef struct gft_tuning {
                                  above every graph to run each query on one CTA) */
     uint32_t direction;       /* BFS: 0 = direction-optimising when the graph is
                                  marked symmetric, 1 = top-down only          */
+    uint32_t cta_small;       /* SSSP on the grid: iterations of at most this
+                                 many vertices run on one CTA while the others
+                                 wait (0 = engine default: 256 on graphs of
+                                 uniform degree, never on skewed ones;
+                                 UINT32_MAX = never) */
 } gft_tuning;
 
 /* ---------------------------------------------------------------------------

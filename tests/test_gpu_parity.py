@@ -95,6 +95,24 @@ def test_road_sssp(gft, orc, engine):
             assert orc.check_tree(g.row_start, g.edge_dst, g.edge_data, src, got, par) == 0
 
 
+@pytest.mark.parametrize("cta_small", [2**32 - 1, 64, 2048, 1 << 22], ids=["never", "64", "2048", "all"])
+def test_sssp_small_iterations_on_one_cta(gft, orc, engine, cta_small):
+    """Grid launches hand runs of small iterations to the first CTA and take
+    the loop state back at a grid barrier: distances and the parent tree
+    stay exact whether that never happens, happens for tiny piles only, or
+    for every iteration (hubs of degree >= 32 included)."""
+    for g, hub in ((gft.CSRGraph.road(400, seed=31), 0), (gft.CSRGraph.rmat(16, 16, seed=32, max_weight=255), 32),
+                   (gft.CSRGraph.grid(12, 4000, 2, 50), 0)):
+        dg = g.copy_to_gpu()
+        tune = dict(max_blocks=1 << 30, cta_small=cta_small, hub_degree=hub)
+        for src in g.pick_sources(33, 2):
+            want = orc.sssp(g.row_start, g.edge_dst, g.edge_data, src)
+            for delta in (100, 10000):
+                got, par, _ = _run_sssp(gft, engine, dg, src, delta, tune)
+                np.testing.assert_array_equal(got, want)
+                assert orc.check_tree(g.row_start, g.edge_dst, g.edge_data, src, got, par) == 0
+
+
 def test_unweighted_sssp_is_zero_weight(gft, orc, engine):
     """An unweighted .gr has weight 0 everywhere (calloc'd edge_data in the
     reference), so every reached vertex has distance 0."""
