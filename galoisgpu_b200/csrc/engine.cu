@@ -52,7 +52,39 @@ __global__ void max_degree_kernel(const uint32_t *__restrict__ row_start, uint32
     for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(0xFFFFFFFFu, m, o));
     if ((threadIdx.x & 31) == 0 && m) atomicMax(out, m);
 }
+
+__global__ void interleave_edges(const uint32_t *__restrict__ dst, const int32_t *__restrict__ w, uint32_t m,
+                                 uint2 *__restrict__ out)
+{
+    for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < m; e += gridDim.x * blockDim.x)
+        out[e] = make_uint2(dst[e], (uint32_t)w[e]);
+}
 }  // namespace dev
+
+gft_status ensure_edge_pairs(gft_graph *g, cudaStream_t stream)
+{
+    std::lock_guard<std::mutex> lk(g->pair_mu);
+    DeviceGraph &G = g->g;
+    if (G.edge_dw || !G.edge_data || !G.nedges) return GFT_OK;
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(stream, &cap) != cudaSuccess || cap != cudaStreamCaptureStatusNone) return GFT_OK;
+    DeviceScope device_scope(G.device);
+    GFT_CUDA_TRY(device_scope.err);
+    uint2 *p = nullptr;
+    if (cudaMalloc(&p, (size_t)G.nedges * sizeof(uint2)) != cudaSuccess) {
+        cudaGetLastError();  // no room: queries keep reading the separate arrays
+        return GFT_OK;
+    }
+    dev::interleave_edges<<<148 * 8, 256, 0, stream>>>(G.edge_dst, G.edge_data, G.nedges, p);
+    cudaError_t err = cudaGetLastError();
+    if (err == cudaSuccess) err = cudaStreamSynchronize(stream);
+    if (err != cudaSuccess) {
+        cudaFree(p);
+        return fail(GFT_ERR_CUDA, "interleaving edges: %s", cudaGetErrorString(err));
+    }
+    G.edge_dw = p;  // complete before any query can see it
+    return GFT_OK;
+}
 
 gft_status graph_degree_stats(DeviceGraph &G, cudaStream_t stream)
 {
@@ -301,6 +333,10 @@ void gft_graph_free(gft_graph *g)
         if (g->g.row_start) cudaFree(g->g.row_start);
         if (g->g.edge_dst) cudaFree(g->g.edge_dst);
         if (g->g.edge_data) cudaFree(g->g.edge_data);
+    }
+    if (g->g.edge_dw) {
+        DeviceScope device_scope(g->g.device);
+        cudaFree(g->g.edge_dw);
     }
     delete g;
 }

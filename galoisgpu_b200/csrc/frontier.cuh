@@ -30,6 +30,7 @@ struct TravParams {
     const uint32_t *__restrict__ row_start;
     const uint32_t *__restrict__ edge_dst;
     const int32_t *__restrict__ edge_data;  // SSSP; NULL = every weight 0
+    const uint2 *__restrict__ edge_dw;      // SSSP: (edge_dst, edge_data) interleaved, or NULL
     uint32_t nnodes;
     uint32_t src;
     int32_t *out;       // level / dist
@@ -177,6 +178,7 @@ struct SsspVisitor {
     static constexpr int kBatch = GFT_SSSP_BATCH;  // edges per lane in one flattened step
     const uint32_t *__restrict__ edge_dst;
     const int32_t *__restrict__ edge_data;
+    const uint2 *__restrict__ edge_dw;  // interleaved (dst, weight), or NULL
     unsigned long long *dt;
     uint32_t *far_stamp;
     uint32_t near_tag, far_tag;
@@ -255,10 +257,19 @@ struct SsspVisitor {
                                           unsigned lane)
     {
         uint32_t d[K], w[K];
+        if (edge_dw) {  // one 8-byte load per edge
 #pragma unroll
-        for (int k = 0; k < K; k++) {
-            d[k] = valid[k] ? ld_stream(edge_dst + e[k]) : 0u;
-            w[k] = (valid[k] && edge_data) ? (uint32_t)__ldcs(edge_data + e[k]) : 0u;
+            for (int k = 0; k < K; k++) {
+                const uint2 x = valid[k] ? __ldcs(edge_dw + e[k]) : make_uint2(0, 0);
+                d[k] = x.x;
+                w[k] = x.y;
+            }
+        } else {
+#pragma unroll
+            for (int k = 0; k < K; k++) {
+                d[k] = valid[k] ? ld_stream(edge_dst + e[k]) : 0u;
+                w[k] = (valid[k] && edge_data) ? (uint32_t)__ldcs(edge_data + e[k]) : 0u;
+            }
         }
         relaxK<K>(valid, d, w, o, lane);
     }
@@ -273,8 +284,15 @@ struct SsspVisitor {
     {
         uint4 d = make_uint4(0, 0, 0, 0), w = make_uint4(0, 0, 0, 0);
         if (valid) {
-            d = ld_stream4(edge_dst + e);
-            if (edge_data) w = __ldcs(reinterpret_cast<const uint4 *>(edge_data + e));
+            if (edge_dw) {  // e % 4 == 0: two 16-byte loads of 32-byte-aligned pairs
+                const uint4 a = __ldcs(reinterpret_cast<const uint4 *>(edge_dw + e));
+                const uint4 b = __ldcs(reinterpret_cast<const uint4 *>(edge_dw + e + 2));
+                d = make_uint4(a.x, a.z, b.x, b.z);
+                w = make_uint4(a.y, a.w, b.y, b.w);
+            } else {
+                d = ld_stream4(edge_dst + e);
+                if (edge_data) w = __ldcs(reinterpret_cast<const uint4 *>(edge_data + e));
+            }
         }
         const bool vv[4] = {valid, valid, valid, valid};
         const uint32_t dd[4] = {d.x, d.y, d.z, d.w}, ww[4] = {w.x, w.y, w.z, w.w};
@@ -813,6 +831,7 @@ __device__ __forceinline__ void sssp_body(const TravParams &p, Mode &m, uint32_t
     SsspVisitor vis;
     vis.edge_dst = p.edge_dst;
     vis.edge_data = p.edge_data;
+    vis.edge_dw = p.edge_dw;
     vis.dt = dt;
     vis.far_stamp = p.far_stamp;
     vis.edges = 0;

@@ -44,6 +44,10 @@ struct DeviceGraph {
     bool wrapped = false;
     bool symmetric = false;  // every out-edge is also an in-edge: BFS may run bottom-up
     uint32_t max_degree = 0;  // largest out-degree (set when the graph is created)
+    // (edge_dst[e], edge_data[e]) interleaved, built on the first weighted
+    // SSSP query and owned by the graph even when the arrays above are
+    // wrapped; NULL until then.
+    uint2 *edge_dw = nullptr;
 };
 
 // Lazily grown device allocation owned by an engine.
@@ -123,6 +127,7 @@ struct LaunchShape {
 
 struct gft_graph {
     gft::DeviceGraph g;
+    std::mutex pair_mu;  // guards the lazy build of g.edge_dw
 };
 
 struct gft_engine {
@@ -162,6 +167,10 @@ struct DeviceScope {
 
 // Largest out-degree of a device graph, stored in G.max_degree (one small
 // reduction kernel on `stream`, then a wait).
+// Builds g->g.edge_dw on `stream` if the graph is weighted and it is not
+// there yet, and waits for it; on an allocation failure, or while `stream`
+// is being captured, the graph keeps the separate arrays only.
+gft_status ensure_edge_pairs(gft_graph *g, cudaStream_t stream);
 gft_status graph_degree_stats(DeviceGraph &G, cudaStream_t stream);
 // Graphs whose out-degrees are all at most this many edges have near-equal
 // work per frontier vertex, so a frontier is split into one static chunk
