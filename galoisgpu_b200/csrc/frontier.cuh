@@ -86,6 +86,7 @@ __device__ __forceinline__ void trace_iter(unsigned, unsigned long long) {}
 
 struct BfsVisitor {
     static constexpr int kBatch = GFT_BFS_BATCH;  // edges per lane in one flattened step
+    static constexpr bool kEarlyRow = false;      // owner() loads nothing
     const uint32_t *__restrict__ edge_dst;
     const uint32_t *__restrict__ row_start;  // non-NULL: sum the out-degrees of claimed vertices
     unsigned long long mf;                    // that sum, per lane
@@ -174,8 +175,15 @@ struct SsspOwn {
 // iteration without a separate stamp array or a second atomic.  An
 // improvement above the threshold writes near_tag - 1 and is deduplicated in
 // the far pile with a per-phase stamp.
-struct SsspVisitor {
+//
+// kSolo: the single-query kernel's visitor, which also reads interleaved
+// (dst, weight) pairs when the graph has them and loads a vertex's row
+// alongside its distance; the batched kernel's jobs use the leaner
+// visitor, which keeps that kernel's register budget.
+template <bool kSolo>
+struct SsspVisitorT {
     static constexpr int kBatch = GFT_SSSP_BATCH;  // edges per lane in one flattened step
+    static constexpr bool kEarlyRow = kSolo;       // owner() loads the distance
     const uint32_t *__restrict__ edge_dst;
     const int32_t *__restrict__ edge_data;
     const uint2 *__restrict__ edge_dw;  // interleaved (dst, weight), or NULL
@@ -257,7 +265,7 @@ struct SsspVisitor {
                                           unsigned lane)
     {
         uint32_t d[K], w[K];
-        if (edge_dw) {  // one 8-byte load per edge
+        if (kSolo && edge_dw) {  // one 8-byte load per edge
 #pragma unroll
             for (int k = 0; k < K; k++) {
                 const uint2 x = valid[k] ? __ldcs(edge_dw + e[k]) : make_uint2(0, 0);
@@ -284,7 +292,7 @@ struct SsspVisitor {
     {
         uint4 d = make_uint4(0, 0, 0, 0), w = make_uint4(0, 0, 0, 0);
         if (valid) {
-            if (edge_dw) {  // e % 4 == 0: two 16-byte loads of 32-byte-aligned pairs
+            if (kSolo && edge_dw) {  // e % 4 == 0: two 16-byte loads of 32-byte-aligned pairs
                 const uint4 a = __ldcs(reinterpret_cast<const uint4 *>(edge_dw + e));
                 const uint4 b = __ldcs(reinterpret_cast<const uint4 *>(edge_dw + e + 2));
                 d = make_uint4(a.x, a.z, b.x, b.z);
@@ -390,12 +398,21 @@ __device__ __forceinline__ void expand_frontier(Vis &vis, const TravParams &p, c
             const unsigned idx = i0 + lane;
             const bool has = idx < end;
             const uint32_t u = has ? __ldcg(in + idx) : 0u;
-            Own o = vis.owner(has, u);
+            // A visitor whose owner() loads per-vertex state (the SSSP
+            // distance, the PageRank residual) has the row loaded alongside
+            // it, not after it: both depend only on u, so the loads share
+            // one memory round trip.
             uint32_t start = 0, deg = 0;
-            if (has && vis.active(o)) {
+            if (Vis::kEarlyRow && has) {
                 start = __ldg(p.row_start + u);
                 deg = __ldg(p.row_start + u + 1) - start;
             }
+            Own o = vis.owner(has, u);
+            if (!Vis::kEarlyRow && has && vis.active(o)) {
+                start = __ldg(p.row_start + u);
+                deg = __ldg(p.row_start + u + 1) - start;
+            }
+            if (!(has && vis.active(o))) deg = 0;
             if (deg >= p.hub_degree) {
                 unsigned nch = (deg + kHubChunk - 1) / kHubChunk;
                 unsigned long long old = atomicAdd(hub_ctr, (1ull << 32) | nch);
@@ -708,9 +725,9 @@ __device__ __forceinline__ bool sssp_small(const TravParams &p, Mode &m, const S
 // next threshold.  gwarp/nwarps are the caller's warp numbering for the
 // work split (the grid's, or one CTA's).  Returns 0 to go on, 1 when the
 // traversal is done (both piles empty), -1 when a barrier reported an error.
-template <class Mode>
-__device__ __forceinline__ int sssp_iter(const TravParams &p, Mode &m, SsspVisitor &vis, SsspState &st,
-                                         unsigned n_near, unsigned gwarp, unsigned nwarps)
+template <class Mode, class Vis>
+__device__ __forceinline__ int sssp_iter(const TravParams &p, Mode &m, Vis &vis, SsspState &st, unsigned n_near,
+                                         unsigned gwarp, unsigned nwarps)
 {
     TraversalCtl *ctl = m.ctl;
     const unsigned lane = threadIdx.x & 31;
@@ -735,7 +752,7 @@ __device__ __forceinline__ int sssp_iter(const TravParams &p, Mode &m, SsspVisit
         vis.far_min = kInf;
         vis.fq.queue = sel2(p.far, P);
         vis.fq.len = u32_of(ctl->far_len[P % 3]);
-        expand_frontier<SsspVisitor, SsspOwn>(vis, p, sel2(p.q, I), n_near, u32_of(ctl->claim[slot]),
+        expand_frontier<Vis, SsspOwn>(vis, p, sel2(p.q, I), n_near, u32_of(ctl->claim[slot]),
                                               &ctl->hub[slot].v, pick_grain(n_near, nwarps, p.uniform), gwarp, nwarps,
                                               lane);
         vis.nq.flush(lane);
@@ -746,7 +763,7 @@ __device__ __forceinline__ int sssp_iter(const TravParams &p, Mode &m, SsspVisit
         const unsigned long long hv = m.ld64(&ctl->hub[slot].v);
         if (hv) {
             vis.far_min = kInf;
-            expand_hubs<SsspVisitor, SsspOwn>(vis, p, (unsigned)(hv >> 32), (unsigned)hv,
+            expand_hubs<Vis, SsspOwn>(vis, p, (unsigned)(hv >> 32), (unsigned)hv,
                                               u32_of(ctl->hub_claim[slot]), gwarp, nwarps, lane);
             vis.nq.flush(lane);
             vis.fq.flush(lane);
@@ -807,7 +824,11 @@ __device__ __forceinline__ int sssp_iter(const TravParams &p, Mode &m, SsspVisit
     return 0;
 }
 
-template <class Mode>
+// kSolo: a single query (the persistent grid or the single-CTA kernel):
+// runs of small iterations may go to the first CTA of a grid launch (needs
+// p.cta_small), and the visitor reads interleaved edges.  The batched
+// kernel's jobs use the lean body.
+template <class Mode, bool kSolo = false>
 __device__ __forceinline__ void sssp_body(const TravParams &p, Mode &m, uint32_t *near_buf, uint32_t *far_buf)
 {
     TraversalCtl *ctl = m.ctl;
@@ -828,7 +849,7 @@ __device__ __forceinline__ void sssp_body(const TravParams &p, Mode &m, uint32_t
     }
     if (!m.sync()) return;
 
-    SsspVisitor vis;
+    SsspVisitorT<kSolo> vis;
     vis.edge_dst = p.edge_dst;
     vis.edge_data = p.edge_data;
     vis.edge_dw = p.edge_dw;
@@ -849,7 +870,7 @@ __device__ __forceinline__ void sssp_body(const TravParams &p, Mode &m, uint32_t
     SsspState st{p.delta, 0, 0};
     for (;;) {
         const unsigned n_near = m.ld(u32_of(ctl->qlen[st.I % 3]));
-        if (Mode::kGrid && p.cta_small && sssp_small(p, m, st, n_near)) {
+        if (kSolo && Mode::kGrid && p.cta_small && sssp_small(p, m, st, n_near)) {
             // Small iterations: the first CTA runs them alone, with
             // __syncthreads as the barrier, while the other CTAs wait at the
             // grid barrier below; it hands the loop state over there.

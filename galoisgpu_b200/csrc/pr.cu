@@ -55,6 +55,7 @@ struct PrOwn {
 // Init: every vertex adds (float)(1.0 / outdeg) along its edges.
 struct PrInitVisitor {
     static constexpr int kBatch = 2;
+    static constexpr bool kEarlyRow = false;  // owner() reads only the degree
     const uint32_t *__restrict__ row_start;
     const uint32_t *__restrict__ edge_dst;
     float *residual;
@@ -116,6 +117,7 @@ struct PrInitVisitor {
 // themselves, so no push waits for the residual it changed.
 struct PrVisitor {
     static constexpr int kBatch = 4;
+    static constexpr bool kEarlyRow = true;  // owner() pops the residual
     const uint32_t *__restrict__ row_start;
     const uint32_t *__restrict__ edge_dst;
     float *rank, *residual, *hub_upd;

@@ -58,7 +58,7 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) sssp_persistent(TravParam
     const unsigned tid = blockIdx.x * BLOCK + threadIdx.x, nthreads = gridDim.x * BLOCK;
     GridMode m{{&ctl->barrier.v, u32_of(ctl->release), &ctl->error, &ctl->error_where, gridDim.x, 0, p.timeout_ns},
                ctl, tid, nthreads, tid / 32, nthreads / 32};
-    sssp_body(p, m, s_near[threadIdx.x >> 5], s_far[threadIdx.x >> 5]);
+    sssp_body<GridMode, true>(p, m, s_near[threadIdx.x >> 5], s_far[threadIdx.x >> 5]);
 }
 
 // ---------------------------------------------------------------------------
@@ -107,7 +107,7 @@ __global__ void __launch_bounds__(kCtaBlock, 1) sssp_single_cta(TravParams p)
     TraversalCtl *gctl = p.ctl;
     p.ctl = &s_ctl;
     CtaMode m{&s_ctl, threadIdx.x, kCtaBlock, threadIdx.x >> 5, kCtaBlock / 32, 0};
-    sssp_body(p, m, s_near[threadIdx.x >> 5], s_far[threadIdx.x >> 5]);
+    sssp_body<CtaMode, true>(p, m, s_near[threadIdx.x >> 5], s_far[threadIdx.x >> 5]);
     __syncthreads();
     if (threadIdx.x == 0) publish_cta_result(s_ctl, gctl);
 }
