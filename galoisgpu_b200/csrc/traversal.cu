@@ -263,7 +263,11 @@ gft_status run_traversal(bool is_sssp, gft_engine *e, const gft_graph *g, uint32
     if (!d_out) return fail(GFT_ERR_INVALID_ARG, "%s: output pointer is NULL", what);
     if (src >= G.nnodes) return fail(GFT_ERR_INVALID_ARG, "%s: source %u out of range (nnodes %u)", what, src, G.nnodes);
     if (is_sssp && delta <= 0) return fail(GFT_ERR_INVALID_ARG, "%s: delta must be > 0 (got %d)", what, delta);
-    if (is_sssp && G.edge_data && !G.edge_dw) GFT_TRY(ensure_edge_pairs(const_cast<gft_graph *>(g), stream));
+    // Graphs the engine owns get the interleaved edge pairs; a wrapped graph
+    // (the caller's arrays, adopted without a copy) keeps that promise and
+    // is read from the separate arrays.
+    if (is_sssp && G.edge_data && !G.edge_dw && !G.wrapped)
+        GFT_TRY(ensure_edge_pairs(const_cast<gft_graph *>(g), stream));
     Tune t = resolve_tuning(tune, is_sssp);
     const void *kern = is_sssp ? sssp_kernel_for(t.block) : bfs_kernel_for(t.block);
     if (!kern) return fail(GFT_ERR_INVALID_ARG, "%s: block_threads must be 256, 512 or 1024", what);
