@@ -77,6 +77,7 @@ class Tuning(C.Structure):
         ("group_min_nodes", C.c_uint32),
         ("direction", C.c_uint32),
         ("cta_small", C.c_uint32),
+        ("fuse_budget", C.c_uint32),
     ]
 
 

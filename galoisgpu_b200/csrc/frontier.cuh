@@ -53,6 +53,7 @@ struct TravParams {
     int dir_opt;  // BFS: direction-optimising (graph marked symmetric)
     int uniform;  // every out-degree <= kUniformDegree: static chunks
     uint32_t cta_small;  // SSSP on the grid: iterations of at most this many vertices run on one CTA (0 = never)
+    uint32_t fuse;       // SSSP: near vertices a warp may expand itself in the iteration that found them (0 = none)
 };
 
 // ---------------------------------------------------------------------------
@@ -184,6 +185,7 @@ template <bool kSolo>
 struct SsspVisitorT {
     static constexpr int kBatch = GFT_SSSP_BATCH;  // edges per lane in one flattened step
     static constexpr bool kEarlyRow = kSolo;       // owner() loads the distance
+    static constexpr bool kFuse = kSolo;           // warps may expand the near vertices they found
     const uint32_t *__restrict__ edge_dst;
     const int32_t *__restrict__ edge_data;
     const uint2 *__restrict__ edge_dw;  // interleaved (dst, weight), or NULL
@@ -382,9 +384,47 @@ __device__ __forceinline__ void flatten_edges(Vis &vis, uint32_t start, uint32_t
     }
 }
 
-// Expands the frontier `in[0, n)` in chunks of `grain` vertices.  Vertices
-// of degree >= hub_degree are recorded in the hub list for the grid-wide hub
-// phase instead.
+// Expands one vertex per lane (`has` false on idle lanes): degree >= 32 by
+// the whole warp, smaller lists flattened across it; vertices of degree >=
+// hub_degree go to the hub list for the grid-wide hub phase.
+template <class Vis, class Own>
+__device__ __forceinline__ void expand_lanes(Vis &vis, const TravParams &p, bool has, uint32_t u,
+                                             unsigned long long *hub_ctr, unsigned lane)
+{
+    // A visitor whose owner() loads per-vertex state (the SSSP distance, the
+    // PageRank residual) has the row loaded alongside it, not after it: both
+    // depend only on u, so the loads share one memory round trip.
+    uint32_t start = 0, deg = 0;
+    if (Vis::kEarlyRow && has) {
+        start = __ldg(p.row_start + u);
+        deg = __ldg(p.row_start + u + 1) - start;
+    }
+    Own o = vis.owner(has, u);
+    if (!Vis::kEarlyRow && has && vis.active(o)) {
+        start = __ldg(p.row_start + u);
+        deg = __ldg(p.row_start + u + 1) - start;
+    }
+    if (!(has && vis.active(o))) deg = 0;
+    if (deg >= p.hub_degree) {
+        unsigned nch = (deg + kHubChunk - 1) / kHubChunk;
+        unsigned long long old = atomicAdd(hub_ctr, (1ull << 32) | nch);
+        unsigned h = (unsigned)(old >> 32);
+        if (h < p.hub_cap) p.hubs[h] = make_uint2(u, (unsigned)old);
+        else raise_error(&p.ctl->error, &p.ctl->error_where, GFT_ERR_OVERFLOW, h);
+        deg = 0;
+    }
+    unsigned m = __ballot_sync(kFull, deg >= 32);
+    while (m) {
+        const int l = __ffs(m) - 1;
+        m &= m - 1;
+        const uint32_t s = __shfl_sync(kFull, start, l), d = __shfl_sync(kFull, deg, l);
+        warp_range(vis, s, d, vis.shfl(o, l), lane);
+    }
+    if (deg >= 32) deg = 0;
+    flatten_edges<Vis::kBatch>(vis, start, deg, o, lane);
+}
+
+// Expands the frontier `in[0, n)` in chunks of `grain` vertices.
 template <class Vis, class Own>
 __device__ __forceinline__ void expand_frontier(Vis &vis, const TravParams &p, const uint32_t *in, uint32_t n,
                                                 unsigned *claim, unsigned long long *hub_ctr, unsigned grain,
@@ -398,38 +438,7 @@ __device__ __forceinline__ void expand_frontier(Vis &vis, const TravParams &p, c
             const unsigned idx = i0 + lane;
             const bool has = idx < end;
             const uint32_t u = has ? __ldcg(in + idx) : 0u;
-            // A visitor whose owner() loads per-vertex state (the SSSP
-            // distance, the PageRank residual) has the row loaded alongside
-            // it, not after it: both depend only on u, so the loads share
-            // one memory round trip.
-            uint32_t start = 0, deg = 0;
-            if (Vis::kEarlyRow && has) {
-                start = __ldg(p.row_start + u);
-                deg = __ldg(p.row_start + u + 1) - start;
-            }
-            Own o = vis.owner(has, u);
-            if (!Vis::kEarlyRow && has && vis.active(o)) {
-                start = __ldg(p.row_start + u);
-                deg = __ldg(p.row_start + u + 1) - start;
-            }
-            if (!(has && vis.active(o))) deg = 0;
-            if (deg >= p.hub_degree) {
-                unsigned nch = (deg + kHubChunk - 1) / kHubChunk;
-                unsigned long long old = atomicAdd(hub_ctr, (1ull << 32) | nch);
-                unsigned h = (unsigned)(old >> 32);
-                if (h < p.hub_cap) p.hubs[h] = make_uint2(u, (unsigned)old);
-                else raise_error(&p.ctl->error, &p.ctl->error_where, GFT_ERR_OVERFLOW, h);
-                deg = 0;
-            }
-            unsigned m = __ballot_sync(kFull, deg >= 32);
-            while (m) {
-                const int l = __ffs(m) - 1;
-                m &= m - 1;
-                const uint32_t s = __shfl_sync(kFull, start, l), d = __shfl_sync(kFull, deg, l);
-                warp_range(vis, s, d, vis.shfl(o, l), lane);
-            }
-            if (deg >= 32) deg = 0;
-            flatten_edges<Vis::kBatch>(vis, start, deg, o, lane);
+            expand_lanes<Vis, Own>(vis, p, has, u, hub_ctr, lane);
         }
     }
 }
@@ -704,6 +713,25 @@ __device__ __forceinline__ void bfs_body(const TravParams &p, Mode &m, uint32_t 
 // ---------------------------------------------------------------------------
 // SSSP body (near-far)
 // ---------------------------------------------------------------------------
+// Bucket fusion: a warp that pushed v to the near pile in this iteration may
+// expand v itself before the barrier.  It first claims v by swapping v's
+// tag from this iteration's near tag to another value, so that a later
+// improvement of v in the same iteration queues it again (the near-pile
+// test compares against the near tag); it then reads v's distance as the
+// expansion's owner, so no improvement is lost.  False when another warp's
+// claim changed the tag first.  The loop ends: the word only changes by
+// distance decreases and claims.
+__device__ __forceinline__ bool sssp_claim(unsigned long long *dt, uint32_t v, uint32_t near_tag)
+{
+    unsigned long long w = __ldcg(dt + v);
+    while ((uint32_t)w == near_tag) {
+        const unsigned long long old = atomicCAS(dt + v, w, (w & 0xFFFFFFFF00000000ull) | (near_tag - 1));
+        if (old == w) return true;
+        w = old;
+    }
+    return false;
+}
+
 // Near-far loop state: bucket threshold (inclusive), iteration, phase.
 struct SsspState {
     unsigned long long T;
@@ -755,6 +783,23 @@ __device__ __forceinline__ int sssp_iter(const TravParams &p, Mode &m, Vis &vis,
         expand_frontier<Vis, SsspOwn>(vis, p, sel2(p.q, I), n_near, u32_of(ctl->claim[slot]),
                                               &ctl->hub[slot].v, pick_grain(n_near, nwarps, p.uniform), gwarp, nwarps,
                                               lane);
+        if (Vis::kFuse && p.fuse) {
+            // Bucket fusion (as in GraphIt's delta-stepping, Zhang et al.,
+            // CGO 2020): expand up to p.fuse of this warp's fresh near
+            // vertices now, newest first, instead of in the next iteration.
+            unsigned budget = p.fuse;
+            while (vis.nq.count && budget) {
+                const unsigned take = min(32u, vis.nq.count);
+                const unsigned base = vis.nq.count - take;
+                __syncwarp();
+                const uint32_t v = lane < take ? vis.nq.buf[base + lane] : 0u;
+                __syncwarp();
+                vis.nq.count = base;
+                budget = budget > take ? budget - take : 0;
+                const bool mine = lane < take && sssp_claim(p.dt, v, vis.near_tag);
+                expand_lanes<Vis, SsspOwn>(vis, p, mine, v, &ctl->hub[slot].v, lane);
+            }
+        }
         vis.nq.flush(lane);
         vis.fq.flush(lane);
         unsigned fm = warp_min_u32(vis.far_min);

@@ -174,6 +174,13 @@ constexpr uint32_t kDefaultTimeoutMs = 20000;
 // longer over the pile, so only tiny piles gain (road 4096^2: 4.81 ->
 // 4.73 ms at 256, slower from 1024 up; R-MAT gains nothing).
 constexpr uint32_t kDefaultCtaSmall = 256;
+// SSSP near vertices a warp may expand itself in the iteration that found
+// them (bucket fusion), by default on graphs of uniform degree.  Road
+// 4096^2, 3 sources: 4.11 ms without (delta 40000), 3.86 ms at 128 with
+// delta 15000 (iterations 203 -> ~70); road 2048^2 gains ~20%; R-MAT loses
+// (4.0 -> 4.4 ms on RMAT-22), where a warp's chased vertices are hubs'
+// neighbourhoods and unbalance the grid.
+constexpr uint32_t kDefaultFuse = 128;
 // Graphs up to this size run on one CTA by default: their frontiers are
 // small enough for 1024 threads, and a __syncthreads per level is several
 // times cheaper than a grid barrier (BFS on the 256^2 grid: 511 levels).
@@ -206,12 +213,13 @@ struct Tune {
     uint32_t max_blocks;
     uint32_t direction;
     uint32_t cta_small;
+    uint32_t fuse;
 };
 
 Tune resolve_tuning(const gft_tuning *t, bool is_sssp)
 {
     Tune r{is_sssp ? kDefaultBlockSssp : kDefaultBlockBfs, kDefaultBlocksPerSm, kDefaultHubDegree, kDefaultTimeoutMs,
-           -1, 0, 0, 0};
+           -1, 0, 0, 0, 0};
     if (t) {
         if (t->block_threads) r.block = t->block_threads;
         if (t->blocks_per_sm) r.bps = t->blocks_per_sm;
@@ -221,6 +229,7 @@ Tune resolve_tuning(const gft_tuning *t, bool is_sssp)
         r.max_blocks = t->max_blocks;
         r.direction = t->direction;
         r.cta_small = t->cta_small;
+        r.fuse = t->fuse_budget;
     }
     return r;
 }
@@ -347,6 +356,7 @@ gft_status run_traversal(bool is_sssp, gft_engine *e, const gft_graph *g, uint32
     p.uniform = G.max_degree <= kUniformDegree;
     if (is_sssp && !single)
         p.cta_small = t.cta_small == UINT32_MAX ? 0 : t.cta_small ? t.cta_small : p.uniform ? kDefaultCtaSmall : 0;
+    if (is_sssp) p.fuse = t.fuse == UINT32_MAX ? 0 : t.fuse ? t.fuse : p.uniform ? kDefaultFuse : 0;
 
     GFT_CUDA_TRY(cudaMemsetAsync(e->ctl.ptr, 0, sizeof(TraversalCtl), stream));
     void *args[] = {&p};

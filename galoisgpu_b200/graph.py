@@ -274,10 +274,12 @@ class Tune:
     group_min_nodes: int = 0
     direction: int = 0  # BFS: 0 = direction-optimising on graphs marked symmetric, 1 = top-down only
     cta_small: int = 0  # SSSP on the grid: iterations up to this many vertices on one CTA (0 = default, 2**32-1 = never)
+    fuse_budget: int = 0  # SSSP: near vertices a warp expands in the iteration that found them (0 = default, 2**32-1 = never)
 
     def c(self) -> Tuning:
         return Tuning(self.block_threads, self.blocks_per_sm, self.hub_degree, self.timeout_ms, self.test_skip_block,
-                      self.max_blocks, self.group_blocks, self.group_min_nodes, self.direction, self.cta_small)
+                      self.max_blocks, self.group_blocks, self.group_min_nodes, self.direction, self.cta_small,
+                      self.fuse_budget)
 
 
 class Engine:

@@ -113,6 +113,24 @@ def test_sssp_small_iterations_on_one_cta(gft, orc, engine, cta_small):
                 assert orc.check_tree(g.row_start, g.edge_dst, g.edge_data, src, got, par) == 0
 
 
+@pytest.mark.parametrize("fuse", [32, 256, 1 << 20], ids=["fuse32", "fuse256", "fuse-unbounded"])
+@pytest.mark.parametrize("mode", [dict(max_blocks=1 << 30), dict(max_blocks=1), dict(max_blocks=1 << 30, hub_degree=32)],
+                         ids=["grid", "one-cta", "grid-hub32"])
+def test_sssp_bucket_fusion(gft, orc, engine, fuse, mode):
+    """Warps that expand the near vertices they found in the same iteration
+    (claimed by swapping the near tag, so later improvements queue them
+    again) give the same distances and a valid parent tree."""
+    for g in (gft.CSRGraph.road(400, seed=41), gft.CSRGraph.rmat(16, 16, seed=42, max_weight=255),
+              gft.CSRGraph.grid(12, 4000, 3, 50)):
+        dg = g.copy_to_gpu()
+        for src in g.pick_sources(43, 2):
+            want = orc.sssp(g.row_start, g.edge_dst, g.edge_data, src)
+            for delta in (100, 10000):
+                got, par, _ = _run_sssp(gft, engine, dg, src, delta, dict(mode, fuse_budget=fuse))
+                np.testing.assert_array_equal(got, want)
+                assert orc.check_tree(g.row_start, g.edge_dst, g.edge_data, src, got, par) == 0
+
+
 def test_unweighted_sssp_is_zero_weight(gft, orc, engine):
     """An unweighted .gr has weight 0 everywhere (calloc'd edge_data in the
     reference), so every reached vertex has distance 0."""
