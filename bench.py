@@ -8,7 +8,7 @@ A step is one single-source query over a resident seeded graph.  The
 headline workload is SSSP on the 4096^2 road-like grid (16.8 M nodes, 5% of
 edges deleted, 0.1% shortcuts, weights uniform [1, 10000], seed 1, source
 drawn from the seed).  Its delta comes from the tuned parameters
-(galoisgpu_b200/tuned_b200.json, 15000; the reference's default is 10000):
+(galoisgpu_b200/tuned_b200.json, 20000; the reference's default is 10000):
 delta changes only the schedule, never the distances.  The metric is GTEPS =
 E_r / t, E_r the sum of out-degrees of the reached vertices.  Rank 0 prints
 one JSON line.

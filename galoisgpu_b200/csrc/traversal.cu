@@ -175,12 +175,13 @@ constexpr uint32_t kDefaultTimeoutMs = 20000;
 // 4.73 ms at 256, slower from 1024 up; R-MAT gains nothing).
 constexpr uint32_t kDefaultCtaSmall = 256;
 // SSSP near vertices a warp may expand itself in the iteration that found
-// them (bucket fusion), by default on graphs of uniform degree.  Road
-// 4096^2, 3 sources: 4.11 ms without (delta 40000), 3.86 ms at 128 with
-// delta 15000 (iterations 203 -> ~70); road 2048^2 gains ~20%; R-MAT loses
-// (4.0 -> 4.4 ms on RMAT-22), where a warp's chased vertices are hubs'
-// neighbourhoods and unbalance the grid.
-constexpr uint32_t kDefaultFuse = 128;
+// them (bucket fusion, on piles of at most dev::kFuseMaxPile vertices), by
+// default on graphs of uniform degree.  Road 4096^2, 3 sources: 4.11 ms
+// without (delta 40000), 3.66 ms at 256 with delta 20000 (iterations
+// 203 -> ~70); road 2048^2 gains ~20%; R-MAT loses (4.0 -> 4.4 ms on
+// RMAT-22), where a warp's chased vertices are hubs' neighbourhoods and
+// unbalance the grid.
+constexpr uint32_t kDefaultFuse = 256;
 // Graphs up to this size run on one CTA by default: their frontiers are
 // small enough for 1024 threads, and a __syncthreads per level is several
 // times cheaper than a grid barrier (BFS on the 256^2 grid: 511 levels).

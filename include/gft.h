@@ -103,8 +103,10 @@ typedef struct gft_tuning {
                                  UINT32_MAX = never) */
     uint32_t fuse_budget;     /* SSSP: near vertices a warp may expand itself in
                                  the iteration that found them (0 = engine
-                                 default: 128 on graphs of uniform degree,
-                                 never on skewed ones; UINT32_MAX = never)    */
+                                 default: 256 on graphs of uniform degree,
+                                 never on skewed ones; UINT32_MAX = never;
+                                 near piles above 262144 vertices are never
+                                 fused)                                       */
 } gft_tuning;
 
 /* ---------------------------------------------------------------------------
