@@ -85,7 +85,21 @@ __device__ __forceinline__ void trace_iter(unsigned i, unsigned long long info)
 __device__ __forceinline__ void trace_iter(unsigned, unsigned long long) {}
 #endif
 
-struct BfsVisitor {
+// A probe of the BFS visited bitmap.  The grid's bitmap is in global memory
+// and read around L1 (other SMs set its bits); a single-CTA traversal of a
+// small graph keeps it in shared memory, where a probe and a claim cost tens
+// of cycles instead of an L2 round trip each.
+template <bool kLocalBits>
+__device__ __forceinline__ uint32_t ld_bits(const uint32_t *p)
+{
+    if constexpr (kLocalBits)
+        return *(const volatile uint32_t *)p;
+    else
+        return __ldcg(p);
+}
+
+template <bool kLocalBits = false>
+struct BfsVisitorT {
     static constexpr int kBatch = GFT_BFS_BATCH;  // edges per lane in one flattened step
     static constexpr bool kEarlyRow = false;      // owner() loads nothing
     const uint32_t *__restrict__ edge_dst;
@@ -117,7 +131,7 @@ struct BfsVisitor {
     {
         uint32_t word[K];
 #pragma unroll
-        for (int k = 0; k < K; k++) word[k] = valid[k] ? __ldcg(visited + (dst[k] >> 5)) : 0xFFFFFFFFu;
+        for (int k = 0; k < K; k++) word[k] = valid[k] ? ld_bits<kLocalBits>(visited + (dst[k] >> 5)) : 0xFFFFFFFFu;
         bool mine[K];
 #pragma unroll
         for (int k = 0; k < K; k++) {
@@ -162,6 +176,7 @@ struct BfsVisitor {
         visitK<4>(v, dd, oo, lane);
     }
 };
+using BfsVisitor = BfsVisitorT<false>;
 
 struct SsspOwn {
     uint32_t u;
@@ -493,13 +508,14 @@ __device__ __forceinline__ unsigned pick_grain(unsigned n, unsigned nwarps, bool
 // the visited bitmap and own them for the level, so each sets its word's
 // new bits with one plain store; claimed vertices are also queued, so a
 // top-down level can follow.
-__device__ __forceinline__ void bottom_up_level(BfsVisitor &vis, const TravParams &p, unsigned L, unsigned gwarp,
-                                                unsigned nwarps, unsigned lane)
+template <bool kLocalBits>
+__device__ __forceinline__ void bottom_up_level(BfsVisitorT<kLocalBits> &vis, const TravParams &p, unsigned L,
+                                                unsigned gwarp, unsigned nwarps, unsigned lane)
 {
     const uint32_t n = p.nnodes, nwords = (n + 31) >> 5;
     const int32_t cur = (int32_t)L;
     for (uint32_t w = gwarp; w < nwords; w += nwarps) {
-        const uint32_t word = __ldcg(p.visited + w);
+        const uint32_t word = ld_bits<kLocalBits>(p.visited + w);
         if (word == 0xFFFFFFFFu) continue;  // warp uniform
         const uint32_t v = (w << 5) + lane;
         bool found = false;
@@ -581,7 +597,8 @@ struct CtaMode {
 // frontier holds fewer than 1/kBeta of the vertices.
 constexpr unsigned kAlpha = 14, kBeta = 24, kScan = 32;
 
-template <class Mode>
+// kLocalBits: p.visited points to shared memory (one CTA runs the traversal).
+template <class Mode, bool kLocalBits = false>
 __device__ __forceinline__ void bfs_body(const TravParams &p, Mode &m, uint32_t *warp_buf)
 {
     TraversalCtl *ctl = m.ctl;
@@ -605,7 +622,7 @@ __device__ __forceinline__ void bfs_body(const TravParams &p, Mode &m, uint32_t 
     }
     if (!m.sync()) return;
 
-    BfsVisitor vis;
+    BfsVisitorT<kLocalBits> vis;
     vis.edge_dst = p.edge_dst;
     // Skewed graphs sum the claimed vertices' out-degrees for the direction
     // switch; on uniform-degree graphs the frontier's size times the mean
@@ -630,6 +647,19 @@ __device__ __forceinline__ void bfs_body(const TravParams &p, Mode &m, uint32_t 
     unsigned long long n_seen = 0;  // vertices reached so far (uniform-degree estimate)
     unsigned n_prev = 0;            // previous frontier size
     const float n_f = (float)n, E_f = (float)p.nedges, mean_deg = E_f / fmaxf(1.f, n_f);
+    // One CTA (bitmap in shared memory) on a uniform-degree graph: a warp
+    // takes at least as many frontier vertices as one flattened step holds
+    // at the mean degree (32 * kBatch edges).  A small frontier then keeps a
+    // few warps busy with one step each, instead of every warp paying a
+    // step's fixed cost for a handful of vertices; the level's critical path
+    // is the same single step.  (256^2 grid, frontiers of at most 256
+    // vertices: 16 per warp.)
+    const unsigned min_grain =
+        (kLocalBits && p.uniform)
+            ? max(1u, min(32u, 32u * BfsVisitorT<kLocalBits>::kBatch / max(1u, (unsigned)ceilf(mean_deg))))
+            : 1u;
+    // The frontier's out-degree sum is only gathered on skewed graphs.
+    const bool sum_degrees = p.dir_opt && !p.uniform;
     for (;;) {
         const unsigned slot = L % 3, nslot = (L + 1) % 3, rslot = (L + 2) % 3;
         const unsigned n_in = m.ld(u32_of(ctl->qlen[slot]));
@@ -680,21 +710,22 @@ __device__ __forceinline__ void bfs_body(const TravParams &p, Mode &m, uint32_t 
         if (bottom_up) {
             bottom_up_level(vis, p, L, gwarp, nwarps, lane);
         } else {
-            expand_frontier<BfsVisitor, BfsOwn>(vis, p, sel2(p.q, L), n_in, u32_of(ctl->claim[slot]),
-                                                &ctl->hub[slot].v, pick_grain(n_in, nwarps, p.uniform), gwarp, nwarps, lane);
+            const unsigned grain = max(min_grain, pick_grain(n_in, nwarps, p.uniform));
+            expand_frontier<BfsVisitorT<kLocalBits>, BfsOwn>(vis, p, sel2(p.q, L), n_in, u32_of(ctl->claim[slot]),
+                                                             &ctl->hub[slot].v, grain, gwarp, nwarps, lane);
         }
         vis.q.flush(lane);
-        if (p.dir_opt) {
+        if (sum_degrees) {
             warp_add_u32(mf_next, (unsigned)vis.mf, lane);
             vis.mf = 0;
         }
         if (!m.sync()) return;
         const unsigned long long hv = bottom_up ? 0ull : m.ld64(&ctl->hub[slot].v);
         if (hv) {
-            expand_hubs<BfsVisitor, BfsOwn>(vis, p, (unsigned)(hv >> 32), (unsigned)hv, u32_of(ctl->hub_claim[slot]),
-                                            gwarp, nwarps, lane);
+            expand_hubs<BfsVisitorT<kLocalBits>, BfsOwn>(vis, p, (unsigned)(hv >> 32), (unsigned)hv,
+                                                         u32_of(ctl->hub_claim[slot]), gwarp, nwarps, lane);
             vis.q.flush(lane);
-            if (p.dir_opt) {
+            if (sum_degrees) {
                 warp_add_u32(mf_next, (unsigned)vis.mf, lane);
                 vis.mf = 0;
             }

@@ -81,17 +81,25 @@ __device__ __forceinline__ void publish_cta_result(const TraversalCtl &s, Traver
     g->reached = s.reached;
 }
 
+// Graphs of at most this many vertices keep the BFS visited bitmap in the
+// CTA's shared memory (16 KB): every probe and claim of a level then stays
+// on the SM.
+constexpr uint32_t kCtaLocalBitsNodes = 1u << 17;
+
+template <bool kLocalBits>
 __global__ void __launch_bounds__(kCtaBlock, 1) bfs_single_cta(TravParams p)
 {
     __shared__ TraversalCtl s_ctl;
     __shared__ uint32_t s_buf[kCtaBlock / 32][kQueueBuf];
+    __shared__ uint32_t s_bits[kLocalBits ? kCtaLocalBitsNodes / 32 : 1];
     for (unsigned i = threadIdx.x; i < sizeof(TraversalCtl) / 4; i += kCtaBlock)
         reinterpret_cast<unsigned *>(&s_ctl)[i] = 0;
     __syncthreads();
     TraversalCtl *gctl = p.ctl;
     p.ctl = &s_ctl;
+    if (kLocalBits) p.visited = s_bits;  // bfs_body clears the first (nnodes + 31) / 32 words
     CtaMode m{&s_ctl, threadIdx.x, kCtaBlock, threadIdx.x >> 5, kCtaBlock / 32, 0};
-    bfs_body(p, m, s_buf[threadIdx.x >> 5]);
+    bfs_body<CtaMode, kLocalBits>(p, m, s_buf[threadIdx.x >> 5]);
     __syncthreads();
     if (threadIdx.x == 0) publish_cta_result(s_ctl, gctl);
 }
@@ -294,7 +302,9 @@ gft_status run_traversal(bool is_sssp, gft_engine *e, const gft_graph *g, uint32
         shape.blocks = 1;
         shape.blocks_per_sm = 1;
         shape.sms = e->sms;
-        kern = is_sssp ? (const void *)dev::sssp_single_cta : (const void *)dev::bfs_single_cta;
+        kern = is_sssp                                   ? (const void *)dev::sssp_single_cta
+               : G.nnodes <= dev::kCtaLocalBitsNodes ? (const void *)dev::bfs_single_cta<true>
+                                                     : (const void *)dev::bfs_single_cta<false>;
     } else {
         GFT_TRY(resolve_shape(e, kern, (int)t.block, (int)t.bps, 0, &shape));
         if (t.max_blocks && (uint32_t)shape.blocks > t.max_blocks) shape.blocks = (int)t.max_blocks;

@@ -84,6 +84,22 @@ def test_rmat_bfs_sssp(gft, orc, engine, tune):
             assert orc.check_tree(g.row_start, g.edge_dst, g.edge_data, src, got, par) == 0
 
 
+@pytest.mark.parametrize("side", [362, 363], ids=["bitmap-in-shared", "bitmap-in-global"])
+def test_one_cta_bfs_either_side_of_the_shared_bitmap_limit(gft, orc, engine, side):
+    """A one-CTA BFS keeps its visited bitmap in shared memory for graphs of
+    at most 2^17 vertices (362^2 = 131,044) and in global memory above
+    (363^2 = 131,769); levels and parent trees match the oracle on both
+    sides, top-down and with the direction switch."""
+    g = gft.CSRGraph.road(side, seed=7)
+    dg = g.copy_to_gpu()
+    for src in g.pick_sources(8, 2):
+        want = orc.bfs(g.row_start, g.edge_dst, src)
+        for tune in (dict(max_blocks=1), dict(max_blocks=1, direction=1)):
+            got, par, _ = _run_bfs(gft, engine, dg, src, tune)
+            np.testing.assert_array_equal(got, want)
+            assert orc.check_tree(g.row_start, g.edge_dst, None, src, got, par) == 0
+
+
 def test_road_sssp(gft, orc, engine):
     g = gft.CSRGraph.road(512, seed=1)
     dg = g.copy_to_gpu()
