@@ -104,6 +104,129 @@ __global__ void __launch_bounds__(kCtaBlock, 1) bfs_single_cta(TravParams p)
     if (threadIdx.x == 0) publish_cta_result(s_ctl, gctl);
 }
 
+// ---------------------------------------------------------------------------
+// One CTA, a thread per frontier vertex: BFS on small graphs of uniform low
+// degree (grids, road networks).  Their levels are many and their frontiers
+// a few hundred vertices, so a level costs its critical path, and the
+// general kernel's balancing (prefix sums and shuffle searches over the
+// warp's edges, per-warp queue buffers) costs more than the few edges it
+// balances.  Here a thread walks its vertex's at most kUniformDegree edges
+// four at a time.  The visited bitmap and the first kLaneQueueHead entries of
+// both frontier queues live in shared memory; a queue's later entries go to
+// the engine's global queue at the same index.  A level is: row pair and
+// edge loads, probes and claims in shared memory, one shared atomic per warp
+// step for the appends, one __syncthreads.  Always top-down: levels are the
+// same in either direction, and these graphs' frontiers stay small.
+// ---------------------------------------------------------------------------
+constexpr uint32_t kLaneQueueHead = 16384;
+constexpr size_t kLaneSmemBytes = (kCtaLocalBitsNodes / 32 + 2 * (size_t)kLaneQueueHead) * 4;
+
+__global__ void __launch_bounds__(kCtaBlock, 1) bfs_cta_lanes(TravParams p)
+{
+    extern __shared__ __align__(16) uint32_t s_lane[];
+    uint32_t *bits = s_lane;
+    uint32_t *const head0 = bits + kCtaLocalBitsNodes / 32, *const head1 = head0 + kLaneQueueHead;
+    __shared__ unsigned s_len[3];
+    __shared__ unsigned s_err;
+    const unsigned tid = threadIdx.x, lane = tid & 31;
+    const uint32_t n = p.nnodes, nwords = (n + 31) >> 5;
+    for (uint32_t v = tid; v < n; v += kCtaBlock) {
+        p.out[v] = v == p.src ? 0 : (int32_t)kInf;
+        if (p.parent) p.parent[v] = v == p.src ? p.src : GFT_NO_PARENT;
+    }
+    for (uint32_t w = tid; w < nwords; w += kCtaBlock) bits[w] = w == (p.src >> 5) ? 1u << (p.src & 31) : 0u;
+    if (tid == 0) {
+        head0[0] = p.src;
+        s_len[0] = 1;
+        s_len[1] = 0;
+        s_len[2] = 0;
+        s_err = 0;
+    }
+    __syncthreads();
+
+    unsigned long long edges = 0, claimed = 0;
+    unsigned L = 0;
+    for (;;) {
+        // Lengths are triple-buffered: slot L % 3 is read by every thread
+        // here, slot (L + 1) % 3 collects this level's appends, and slot
+        // (L + 2) % 3 (read at the top of the previous level, before its
+        // barrier) is cleared for the next level.
+        const unsigned n_in = *(volatile unsigned *)&s_len[L % 3];
+        if (n_in == 0) break;
+        if (tid == 0) s_len[(L + 2) % 3] = 0;
+        unsigned *len_next = &s_len[(L + 1) % 3];
+        const uint32_t *in_head = (L & 1) ? head1 : head0, *in_tail = sel2(p.q, L);
+        uint32_t *out_head = (L & 1) ? head0 : head1, *out_tail = sel2(p.q, L + 1);
+        const int32_t next_level = (int32_t)L + 1;
+        for (unsigned base = tid - lane; base < n_in; base += kCtaBlock) {  // warp-uniform trip count
+            const unsigned i = base + lane;
+            uint32_t u = 0, s = 0, deg = 0;
+            if (i < n_in) {
+                u = i < kLaneQueueHead ? in_head[i] : __ldcg(in_tail + i);
+                s = __ldg(p.row_start + u);
+                deg = __ldg(p.row_start + u + 1) - s;
+            }
+            const unsigned max_deg = __reduce_max_sync(kFull, deg);
+            for (unsigned j = 0; j < max_deg; j += 4) {
+                uint32_t v[4];
+#pragma unroll
+                for (int k = 0; k < 4; k++) v[k] = j + k < deg ? ld_stream(p.edge_dst + s + j + k) : 0u;
+                bool mine[4];
+                unsigned mask[4], total = 0;
+#pragma unroll
+                for (int k = 0; k < 4; k++) {
+                    mine[k] = false;
+                    if (j + k < deg) {
+                        edges++;
+                        if (v[k] < n) {
+                            uint32_t *w = bits + (v[k] >> 5);
+                            const uint32_t b = 1u << (v[k] & 31);
+                            if (!(*(volatile uint32_t *)w & b)) mine[k] = !(atomicOr(w, b) & b);
+                        } else {
+                            atomicCAS(&s_err, 0u, (unsigned)GFT_ERR_FORMAT);
+                        }
+                    }
+                    mask[k] = __ballot_sync(kFull, mine[k]);
+                    total += __popc(mask[k]);
+                }
+                if (total == 0) continue;  // warp uniform
+                unsigned at = 0;
+                if (lane == 0) at = atomicAdd(len_next, total);
+                at = __shfl_sync(kFull, at, 0);
+#pragma unroll
+                for (int k = 0; k < 4; k++) {
+                    if (mine[k]) {
+                        // Each vertex is claimed once, so a level appends
+                        // fewer than qcap = nnodes entries.
+                        const unsigned slot = at + __popc(mask[k] & lanemask_lt());
+                        if (slot < kLaneQueueHead)
+                            out_head[slot] = v[k];
+                        else if (slot < p.qcap)
+                            out_tail[slot] = v[k];
+                        else
+                            atomicCAS(&s_err, 0u, (unsigned)GFT_ERR_OVERFLOW);
+                        p.out[v[k]] = next_level;
+                        if (p.parent) p.parent[v[k]] = u;
+                        claimed++;
+                    }
+                    at += __popc(mask[k]);
+                }
+            }
+        }
+        // Every thread gets the same answer, so all leave at the same level.
+        const bool failed = __syncthreads_or(*(volatile unsigned *)&s_err != 0);
+        L++;
+        if (failed) break;
+    }
+    warp_add_u64(&p.ctl->edges, edges, lane);
+    warp_add_u64(&p.ctl->reached, claimed, lane);
+    if (tid == 0) {
+        p.ctl->levels = L;
+        p.ctl->iterations = L + 1;  // barriers, as the general kernel counts them
+        if (s_err) p.ctl->error = s_err;
+    }
+}
+
 __global__ void __launch_bounds__(kCtaBlock, 1) sssp_single_cta(TravParams p)
 {
     __shared__ TraversalCtl s_ctl;
@@ -297,14 +420,23 @@ gft_status run_traversal(bool is_sssp, gft_engine *e, const gft_graph *g, uint32
     const bool single = t.max_blocks == 1 || (t.max_blocks == 0 && t.skip < 0 && G.nnodes <= kCtaMaxNodes &&
                                               G.nedges <= kCtaMaxEdges);
     LaunchShape shape;
+    size_t dyn_smem = 0;
     if (single) {
         shape.block_threads = dev::kCtaBlock;
         shape.blocks = 1;
         shape.blocks_per_sm = 1;
         shape.sms = e->sms;
-        kern = is_sssp                                   ? (const void *)dev::sssp_single_cta
-               : G.nnodes <= dev::kCtaLocalBitsNodes ? (const void *)dev::bfs_single_cta<true>
-                                                     : (const void *)dev::bfs_single_cta<false>;
+        if (is_sssp) {
+            kern = (const void *)dev::sssp_single_cta;
+        } else if (G.nnodes <= dev::kCtaLocalBitsNodes && G.max_degree <= kUniformDegree) {
+            // Thread per frontier vertex, bitmap and queue heads in shared memory.
+            kern = (const void *)dev::bfs_cta_lanes;
+            dyn_smem = dev::kLaneSmemBytes;
+            GFT_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn_smem));
+        } else {
+            kern = G.nnodes <= dev::kCtaLocalBitsNodes ? (const void *)dev::bfs_single_cta<true>
+                                                       : (const void *)dev::bfs_single_cta<false>;
+        }
     } else {
         GFT_TRY(resolve_shape(e, kern, (int)t.block, (int)t.bps, 0, &shape));
         if (t.max_blocks && (uint32_t)shape.blocks > t.max_blocks) shape.blocks = (int)t.max_blocks;
@@ -373,7 +505,7 @@ gft_status run_traversal(bool is_sssp, gft_engine *e, const gft_graph *g, uint32
     void *args[] = {&p};
     GFT_CUDA_TRY(cudaEventRecord(e->ev0, stream));
     if (single)
-        GFT_CUDA_TRY(cudaLaunchKernel(kern, dim3(1), dim3(shape.block_threads), args, 0, stream));
+        GFT_CUDA_TRY(cudaLaunchKernel(kern, dim3(1), dim3(shape.block_threads), args, dyn_smem, stream));
     else
         GFT_CUDA_TRY(cudaLaunchCooperativeKernel(kern, dim3(shape.blocks), dim3(shape.block_threads), args, 0, stream));
     GFT_CUDA_TRY(cudaEventRecord(e->ev1, stream));

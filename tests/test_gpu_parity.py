@@ -100,6 +100,39 @@ def test_one_cta_bfs_either_side_of_the_shared_bitmap_limit(gft, orc, engine, si
             assert orc.check_tree(g.row_start, g.edge_dst, None, src, got, par) == 0
 
 
+def test_one_cta_bfs_frontier_beyond_the_shared_queue_head(gft, orc, engine):
+    """Small uniform-degree graphs run a thread per frontier vertex on one
+    CTA, with the first 16,384 entries of each frontier queue in shared
+    memory and the rest in global memory.  A random graph of 120,000
+    vertices and degree <= 32 has levels of tens of thousands of vertices,
+    so both parts of the queue carry vertices; levels and parents stay
+    exact."""
+    rng = np.random.default_rng(12)
+    n, m = 120_000, 240_000
+    u = rng.integers(0, n, m, dtype=np.int64)
+    v = rng.integers(0, n, m, dtype=np.int64)
+    keep = u != v
+    a = np.concatenate([u[keep], v[keep]])
+    b = np.concatenate([v[keep], u[keep]])
+    key = np.unique(a * n + b)
+    src_of, dst = (key // n).astype(np.uint32), (key % n).astype(np.uint32)
+    rs = np.zeros(n + 1, dtype=np.uint32)
+    np.cumsum(np.bincount(src_of, minlength=n), out=rs[1:])
+    assert int(np.diff(rs.astype(np.int64)).max()) <= 32 and len(dst) <= 1 << 19
+    g = gft.CSRGraph(rs, dst, None)
+    dg = g.copy_to_gpu()
+    for src in g.pick_sources(13, 2):
+        want = orc.bfs(rs, dst, src)
+        reached = want != np.iinfo(np.int32).max
+        assert np.bincount(want[reached]).max() > 16384
+        for tune in (None, dict(max_blocks=1)):
+            got, par, r = _run_bfs(gft, engine, dg, src, tune)
+            np.testing.assert_array_equal(got, want)
+            assert orc.check_tree(rs, dst, None, src, got, par) == 0
+            assert r["grid_blocks"] == 1
+            assert r["vertices_reached"] == int(reached.sum()) - 1  # the source is not counted
+
+
 def test_road_sssp(gft, orc, engine):
     g = gft.CSRGraph.road(512, seed=1)
     dg = g.copy_to_gpu()
