@@ -313,6 +313,12 @@ def bench_workload(gft, name: str, steps: int, warmup: int, d, dev: int, headlin
     alg_bytes = algorithmic_bytes(app, v_sum, e_alg) / k
     achieved = alg_bytes / (kernel_ms * 1e-3) / 1e9
     kname = f"{app}_persistent"
+    if qstats and qstats[0]["grid_blocks"] == 1:
+        # Small graphs run on one CTA: BFS on a uniform-degree graph of at
+        # most 2^17 vertices takes the thread-per-vertex kernel.
+        max_deg = int(np.diff(host.row_start.astype(np.int64)).max(initial=0))
+        kname = ("sssp_single_cta" if app == "sssp" else
+                 "bfs_cta_lanes" if dg.nnodes <= 1 << 17 and max_deg <= 32 else "bfs_single_cta")
     traffic, traffic_src = profile_traffic(name, kname)
     res = {
         "name": name,

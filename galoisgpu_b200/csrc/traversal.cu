@@ -63,7 +63,7 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) sssp_persistent(TravParam
 
 // ---------------------------------------------------------------------------
 // Single-CTA kernels for small graphs.  A small graph's frontiers are small
-// and its levels many (the 256^2 grid: 511 levels of at most 512 vertices),
+// and its levels many (the 256^2 grid: 511 levels of at most 256 vertices),
 // so a grid barrier per level dominates.  One CTA runs the whole traversal
 // with its control block in shared memory and __syncthreads as the barrier
 // (CtaMode, as the batched kernel's small jobs), then copies the results to
@@ -111,7 +111,8 @@ __global__ void __launch_bounds__(kCtaBlock, 1) bfs_single_cta(TravParams p)
 // general kernel's balancing (prefix sums and shuffle searches over the
 // warp's edges, per-warp queue buffers) costs more than the few edges it
 // balances.  Here a thread walks its vertex's at most kUniformDegree edges
-// four at a time.  The visited bitmap and the first kLaneQueueHead entries of
+// four at a time (read through L1: a level's rows sit next to the previous
+// level's on these graphs).  The visited bitmap and the first kLaneQueueHead entries of
 // both frontier queues live in shared memory; a queue's later entries go to
 // the engine's global queue at the same index.  A level is: row pair and
 // edge loads, probes and claims in shared memory, one shared atomic per warp
@@ -170,22 +171,27 @@ __global__ void __launch_bounds__(kCtaBlock, 1) bfs_cta_lanes(TravParams p)
             for (unsigned j = 0; j < max_deg; j += 4) {
                 uint32_t v[4];
 #pragma unroll
-                for (int k = 0; k < 4; k++) v[k] = j + k < deg ? ld_stream(p.edge_dst + s + j + k) : 0u;
+                for (int k = 0; k < 4; k++) v[k] = j + k < deg ? __ldg(p.edge_dst + s + j + k) : 0u;
+                // The four claims go out together, with no probe first: a
+                // shared-memory atomic costs about what a load does, and
+                // this keeps one shared round trip per step (road 362^2:
+                // 5% faster than probe-then-claim per edge).
                 bool mine[4];
-                unsigned mask[4], total = 0;
 #pragma unroll
                 for (int k = 0; k < 4; k++) {
                     mine[k] = false;
                     if (j + k < deg) {
                         edges++;
-                        if (v[k] < n) {
-                            uint32_t *w = bits + (v[k] >> 5);
-                            const uint32_t b = 1u << (v[k] & 31);
-                            if (!(*(volatile uint32_t *)w & b)) mine[k] = !(atomicOr(w, b) & b);
-                        } else {
+                        const uint32_t b = 1u << (v[k] & 31);
+                        if (v[k] < n)
+                            mine[k] = !(atomicOr(bits + (v[k] >> 5), b) & b);
+                        else
                             atomicCAS(&s_err, 0u, (unsigned)GFT_ERR_FORMAT);
-                        }
                     }
+                }
+                unsigned mask[4], total = 0;
+#pragma unroll
+                for (int k = 0; k < 4; k++) {
                     mask[k] = __ballot_sync(kFull, mine[k]);
                     total += __popc(mask[k]);
                 }
