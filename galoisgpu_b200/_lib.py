@@ -194,6 +194,8 @@ _SIGS: dict[str, tuple] = {
     "gft_sssp": (C.c_int, [_P, _P, C.c_uint32, C.c_int32, _P, _P, C.POINTER(Tuning), _P, C.POINTER(Stats)]),
     "gft_bfs_host": (C.c_int, [_P, _P, C.c_uint32, _P, _P, C.POINTER(Tuning), _P, C.POINTER(Stats)]),
     "gft_sssp_host": (C.c_int, [_P, _P, C.c_uint32, C.c_int32, _P, _P, C.POINTER(Tuning), _P, C.POINTER(Stats)]),
+    "gft_bfs_host_many": (C.c_int, [_P, _P, _P, C.c_uint32, _P, C.POINTER(Tuning), _P, _P]),
+    "gft_sssp_host_many": (C.c_int, [_P, _P, _P, C.c_uint32, C.c_int32, _P, C.POINTER(Tuning), _P, _P]),
     "gft_reach_stats": (C.c_int, [_P, _P, _P, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
     "gft_cc": (C.c_int, [_P, _P, _P, C.POINTER(Tuning), _P, C.POINTER(Stats), C.POINTER(C.c_uint64)]),
     "gft_cc_host": (C.c_int, [_P, _P, _P, C.POINTER(Tuning), _P, C.POINTER(Stats), C.POINTER(C.c_uint64)]),

@@ -185,6 +185,11 @@ void gft_engine_destroy(gft_engine *e)
     if (e->host_ctl) cudaFreeHost(e->host_ctl);
     if (e->ev0) cudaEventDestroy(e->ev0);
     if (e->ev1) cudaEventDestroy(e->ev1);
+    if (e->copy_stream) cudaStreamSynchronize(e->copy_stream), cudaStreamDestroy(e->copy_stream);
+    for (int i = 0; i < 2; i++) {
+        if (e->result_ready[i]) cudaEventDestroy(e->result_ready[i]);
+        if (e->copy_done[i]) cudaEventDestroy(e->copy_done[i]);
+    }
     delete e;
 }
 

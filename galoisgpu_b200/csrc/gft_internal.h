@@ -139,6 +139,10 @@ struct gft_engine {
     gft::Scratch aux;        // per-call small buffers (e.g. the source id)
     void *host_ctl = nullptr;  // pinned copy of the TraversalCtl read back after a launch
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    // Many-query host calls: results go back to the host on this stream while
+    // the next query runs; created on first use.
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t result_ready[2] = {nullptr, nullptr}, copy_done[2] = {nullptr, nullptr};
     std::mutex mu;
 };
 

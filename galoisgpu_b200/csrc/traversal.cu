@@ -598,6 +598,71 @@ gft_status gft_sssp_host(gft_engine *e, const gft_graph *g, uint32_t src, int32_
     return run_host(true, e, g, src, delta, h_dist, h_parent, tune, stream, stats);
 }
 
+// k queries on one graph with results to the host: query i writes device
+// buffer i % 2, and its copy to row i runs on the engine's copy stream while
+// query i + 1 runs on `stream`.  Query i + 2 waits for copy i before it
+// reuses the buffer.
+static gft_status run_host_many(bool is_sssp, gft_engine *e, const gft_graph *g, const uint32_t *sources, uint32_t k,
+                                int32_t delta, int32_t *h_out, const gft_tuning *tune, void *stream_, gft_stats *stats)
+{
+    const char *what = is_sssp ? "gft_sssp_host_many" : "gft_bfs_host_many";
+    if (!e) return fail(GFT_ERR_INVALID_ARG, "%s: engine is NULL", what);
+    if (k && (!sources || !h_out)) return fail(GFT_ERR_INVALID_ARG, "%s: sources or output pointer is NULL", what);
+    std::lock_guard<std::mutex> lk(e->mu);
+    GFT_TRY(check_engine_graph(e, g));
+    const size_t n = g->g.nnodes;
+    for (uint32_t i = 0; i < k; i++)
+        if (sources[i] >= n)
+            return fail(GFT_ERR_INVALID_ARG, "%s: source %u (query %u) out of range (nnodes %zu)", what, sources[i], i,
+                        n);
+    if (is_sssp && delta <= 0) return fail(GFT_ERR_INVALID_ARG, "%s: delta must be > 0 (got %d)", what, delta);
+    if (k == 0) return GFT_OK;
+    cudaStream_t stream = (cudaStream_t)stream_;
+    DeviceScope device_scope(e->device);
+    GFT_CUDA_TRY(device_scope.err);
+    if (!e->copy_stream) GFT_CUDA_TRY(cudaStreamCreateWithFlags(&e->copy_stream, cudaStreamNonBlocking));
+    for (int b = 0; b < 2; b++) {
+        if (!e->result_ready[b]) GFT_CUDA_TRY(cudaEventCreateWithFlags(&e->result_ready[b], cudaEventDisableTiming));
+        if (!e->copy_done[b]) GFT_CUDA_TRY(cudaEventCreateWithFlags(&e->copy_done[b], cudaEventDisableTiming));
+    }
+    const size_t row = align256(n * 4);
+    GFT_TRY(e->aux.ensure(2 * row));
+    char *base = reinterpret_cast<char *>(e->aux.ptr);
+    gft_status st = GFT_OK;
+    cudaError_t ce = cudaSuccess;
+    for (uint32_t i = 0; i < k && st == GFT_OK && ce == cudaSuccess; i++) {
+        const int b = i & 1;
+        int32_t *d_out = reinterpret_cast<int32_t *>(base + b * row);
+        if (i >= 2) ce = cudaStreamWaitEvent(stream, e->copy_done[b], 0);
+        if (ce != cudaSuccess) break;
+        st = run_traversal(is_sssp, e, g, sources[i], delta, d_out, nullptr, tune, stream, stats ? stats + i : nullptr);
+        if (st != GFT_OK) break;
+        ce = cudaEventRecord(e->result_ready[b], stream);
+        if (ce == cudaSuccess) ce = cudaStreamWaitEvent(e->copy_stream, e->result_ready[b], 0);
+        if (ce == cudaSuccess)
+            ce = cudaMemcpyAsync(h_out + (size_t)i * n, d_out, n * 4, cudaMemcpyDeviceToHost, e->copy_stream);
+        if (ce == cudaSuccess) ce = cudaEventRecord(e->copy_done[b], e->copy_stream);
+    }
+    // No copy into the caller's rows stays in flight after the call.
+    const cudaError_t se = cudaStreamSynchronize(e->copy_stream);
+    if (st != GFT_OK) return st;
+    GFT_CUDA_TRY(ce);
+    GFT_CUDA_TRY(se);
+    return GFT_OK;
+}
+
+gft_status gft_bfs_host_many(gft_engine *e, const gft_graph *g, const uint32_t *sources, uint32_t k, int32_t *h_out,
+                             const gft_tuning *tune, void *stream, gft_stats *stats)
+{
+    return run_host_many(false, e, g, sources, k, 0, h_out, tune, stream, stats);
+}
+
+gft_status gft_sssp_host_many(gft_engine *e, const gft_graph *g, const uint32_t *sources, uint32_t k, int32_t delta,
+                              int32_t *h_out, const gft_tuning *tune, void *stream, gft_stats *stats)
+{
+    return run_host_many(true, e, g, sources, k, delta, h_out, tune, stream, stats);
+}
+
 gft_status gft_reach_stats(const gft_graph *g, const int32_t *d_val, void *stream, uint64_t *v_r, uint64_t *e_r)
 {
     if (!g || !d_val) return fail(GFT_ERR_INVALID_ARG, "gft_reach_stats: null argument");

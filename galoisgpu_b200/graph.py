@@ -472,6 +472,33 @@ class Engine:
         )
         return st.as_dict()
 
+    def _host_many(self, app: str, graph: DeviceGraph, sources, out: np.ndarray, delta: int, tune: Tune | None,
+                   stream) -> list[dict]:
+        src = np.ascontiguousarray(np.asarray(sources, dtype=np.uint32))
+        k = len(src)
+        if out.dtype != np.int32 or not out.flags["C_CONTIGUOUS"] or out.size < k * graph.nnodes:
+            raise ValueError(f"out must be a C-contiguous int32 array of at least {k} x {graph.nnodes} entries")
+        stats = (Stats * max(k, 1))()
+        args = [self._h, graph.handle, C.c_void_p(src.ctypes.data), k]
+        args += [delta] if app == "sssp" else []
+        args += [C.c_void_p(out.ctypes.data), self._tune(tune), _stream_ptr(stream), C.cast(stats, C.c_void_p)]
+        check(getattr(load(), f"gft_{app}_host_many")(*args))
+        return [stats[i].as_dict() for i in range(k)]
+
+    def bfs_host_many(self, graph: DeviceGraph, sources, out: np.ndarray, tune: Tune | None = None,
+                      stream=None) -> list[dict]:
+        """BFS from each of `sources` into the rows of the host array `out`
+        (k x nnodes int32; pinned memory lets each query's copy back overlap
+        the next query).  Row i equals bfs_host from sources[i].  Returns the
+        per-query stats."""
+        return self._host_many("bfs", graph, sources, out, 0, tune, stream)
+
+    def sssp_host_many(self, graph: DeviceGraph, sources, out: np.ndarray, delta: int = DEFAULT_DELTA,
+                       tune: Tune | None = None, stream=None) -> list[dict]:
+        """SSSP from each of `sources` into the rows of the host array `out`,
+        as bfs_host_many."""
+        return self._host_many("sssp", graph, sources, out, delta, tune, stream)
+
 
 class Batch:
     """Many queries in one persistent launch, replayed as a CUDA graph

@@ -238,6 +238,24 @@ GFT_API gft_status gft_bfs_host(gft_engine *e, const gft_graph *g, uint32_t src,
 GFT_API gft_status gft_sssp_host(gft_engine *e, const gft_graph *g, uint32_t src, int32_t delta, int32_t *h_dist,
                          uint32_t *h_parent, const gft_tuning *tune, void *stream, gft_stats *stats);
 
+/* Many single-source queries on one graph, results to host memory.  The
+ * reference runs one source per process and copies node_data back after
+ * each traversal (skelapp/skel.cu:139-174); these calls run the k sources
+ * one after another on `stream`, each exactly as gft_bfs_host /
+ * gft_sssp_host would, but copy a query's results back on an engine-owned
+ * stream while the next query runs (two device result buffers), so the
+ * device->host transfer overlaps the traversal.  h_out holds k rows of
+ * nnodes int32 (row i: levels / distances from sources[i]); it should be
+ * pinned memory, or the copies cannot overlap.  stats: NULL or k entries.
+ * All sources are checked before anything runs.  On an error no copy is
+ * left in flight and the rows of the queries before the failing one are
+ * complete. */
+GFT_API gft_status gft_bfs_host_many(gft_engine *e, const gft_graph *g, const uint32_t *sources, uint32_t k,
+                             int32_t *h_out, const gft_tuning *tune, void *stream, gft_stats *stats);
+GFT_API gft_status gft_sssp_host_many(gft_engine *e, const gft_graph *g, const uint32_t *sources, uint32_t k,
+                              int32_t delta, int32_t *h_out, const gft_tuning *tune, void *stream,
+                              gft_stats *stats);
+
 /* Allocation-free BFS.  No counterpart in the reference: gg_main allocates
  * its worklists on every call (apps/bfs/kernel.cu:389, rt/include/worklist.h:
  * 73-118).  For callers that cannot call cudaMalloc -- code running while

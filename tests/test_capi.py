@@ -53,6 +53,9 @@ def test_null_arguments_are_errors_not_crashes(gft):
     assert lib.gft_bfs(None, None, 0, None, None, None, None, None) == 1
     assert lib.gft_sssp(None, None, 0, 1, None, None, None, None, None) == 1
     assert lib.gft_bfs_host(None, None, 0, None, None, None, None, None) == 1
+    assert lib.gft_bfs_host_many(None, None, None, 1, None, None, None, None) == 1
+    assert lib.gft_sssp_host_many(None, None, None, 1, 1, None, None, None, None) == 1
+    assert b"engine is NULL" in lib.gft_last_error()
     assert lib.gft_graph_info(None, None, None, None) == 1
     lib.gft_graph_free(None)
     lib.gft_engine_destroy(None)

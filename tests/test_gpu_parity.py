@@ -224,6 +224,36 @@ def test_host_api_matches_device_api(gft, orc, engine):
     assert orc.check_tree(g.row_start, g.edge_dst, None, 5, out, par) == 0
 
 
+@pytest.mark.parametrize("app", ["bfs", "sssp"])
+def test_host_many_rows_equal_single_queries(gft, orc, engine, app):
+    """The many-query host calls copy each query's results back while the
+    next query runs, through two device buffers: every row equals the oracle
+    (and so the single-query host call), in pinned and pageable memory, for
+    five sources (both buffers reused), on the grid and on one CTA; no
+    sources is a no-op, and a bad source fails before anything runs."""
+    import torch
+
+    for g in (gft.CSRGraph.road(700, seed=6), gft.CSRGraph.road(100, seed=6)):
+        dg = g.copy_to_gpu()
+        srcs = g.pick_sources(21, 5)
+        want = [orc.sssp(g.row_start, g.edge_dst, g.edge_data, s) if app == "sssp" else
+                orc.bfs(g.row_start, g.edge_dst, s) for s in srcs]
+        run = engine.sssp_host_many if app == "sssp" else engine.bfs_host_many
+        pinned = torch.empty((len(srcs), g.nnodes), dtype=torch.int32, pin_memory=True).numpy()
+        for out in (pinned, np.empty((len(srcs), g.nnodes), dtype=np.int32)):
+            out.fill(-7)
+            st = run(dg, srcs, out)
+            assert len(st) == len(srcs)
+            for i in range(len(srcs)):
+                np.testing.assert_array_equal(out[i], want[i])
+                assert st[i]["levels"] > 0 and st[i]["kernel_ms"] > 0
+        assert run(dg, [], pinned[:0]) == []
+        pinned.fill(-7)
+        with pytest.raises(gft.GftError, match="INVALID_ARG"):
+            run(dg, [srcs[0], g.nnodes], pinned)
+        assert (pinned == -7).all()
+
+
 def test_barrier_timeout_is_reported_and_engine_recovers(gft, orc, engine):
     """One CTA never arrives at the first grid barrier (test hook); the other
     CTAs' bounded waits expire, the call returns GFT_ERR_TIMEOUT and the
