@@ -196,7 +196,7 @@ struct SsspOwn {
 // (dst, weight) pairs when the graph has them and loads a vertex's row
 // alongside its distance; the batched kernel's jobs use the leaner
 // visitor, which keeps that kernel's register budget.
-template <bool kSolo>
+template <bool kSolo, unsigned kQB = kQueueBuf>
 struct SsspVisitorT {
     static constexpr int kBatch = GFT_SSSP_BATCH;  // edges per lane in one flattened step
     static constexpr bool kEarlyRow = kSolo;       // owner() loads the distance
@@ -208,7 +208,7 @@ struct SsspVisitorT {
     uint32_t *far_stamp;
     uint32_t near_tag, far_tag;
     unsigned long long threshold;
-    WarpQueue nq, fq;
+    WarpQueueT<kQB> nq, fq;  // near and far pushes, kQB-entry buffers per warp
     unsigned far_min;
     unsigned long long edges;
     unsigned *err, *err_where;
@@ -910,7 +910,8 @@ __device__ __forceinline__ int sssp_iter(const TravParams &p, Mode &m, Vis &vis,
 // runs of small iterations may go to the first CTA of a grid launch (needs
 // p.cta_small), and the visitor reads interleaved edges.  The batched
 // kernel's jobs use the lean body.
-template <class Mode, bool kSolo = false>
+// near_buf and far_buf: this warp's kQB-entry push buffers.
+template <class Mode, bool kSolo = false, unsigned kQB = kQueueBuf>
 __device__ __forceinline__ void sssp_body(const TravParams &p, Mode &m, uint32_t *near_buf, uint32_t *far_buf)
 {
     TraversalCtl *ctl = m.ctl;
@@ -931,7 +932,7 @@ __device__ __forceinline__ void sssp_body(const TravParams &p, Mode &m, uint32_t
     }
     if (!m.sync()) return;
 
-    SsspVisitorT<kSolo> vis;
+    SsspVisitorT<kSolo, kQB> vis;
     vis.edge_dst = p.edge_dst;
     vis.edge_data = p.edge_data;
     vis.edge_dw = p.edge_dw;

@@ -155,11 +155,13 @@ struct GridSync {
 constexpr unsigned kQueueBuf = GFT_QBUF;
 static_assert(kQueueBuf >= 64 && kQueueBuf % 32 == 0, "queue buffer: a multiple of 32, at least 64");
 
-// Warp-aggregated append to a global queue through a kQueueBuf-entry
-// per-warp shared-memory buffer: one atomic reservation per flush.  `count`
-// is warp uniform.  All 32 lanes must call push() and flush() together.
-struct WarpQueue {
-    uint32_t *buf;       // this warp's kQueueBuf shared-memory slots
+// Warp-aggregated append to a global queue through a CAP-entry per-warp
+// shared-memory buffer: one atomic reservation per flush.  `count` is warp
+// uniform.  All 32 lanes must call push() and flush() together.
+template <unsigned CAP>
+struct WarpQueueT {
+    static_assert(CAP >= 64 && CAP % 32 == 0, "queue buffer: a multiple of 32, at least 64");
+    uint32_t *buf;       // this warp's CAP shared-memory slots
     unsigned count;
     uint32_t *queue;     // global destination
     unsigned *len;       // global length counter
@@ -188,9 +190,10 @@ struct WarpQueue {
         if (mask == 0) return;
         if (p) buf[count + __popc(mask & lanemask_lt())] = item;
         count += __popc(mask);
-        if (count > kQueueBuf - 32) flush(lane);
+        if (count > CAP - 32) flush(lane);
     }
 };
+using WarpQueue = WarpQueueT<kQueueBuf>;
 
 // Inclusive warp prefix sum.
 __device__ __forceinline__ uint32_t warp_incl_sum(uint32_t x, unsigned lane)
