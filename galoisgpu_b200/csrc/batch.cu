@@ -89,14 +89,20 @@ __device__ __forceinline__ void write_result(BatchJob &r, const TraversalCtl &c,
 // each.  A CTA joins phase 2 as soon as its group finds no large job left,
 // so large and small queries overlap.  cursors[0] / cursors[1] hand out
 // small / large jobs; gctl holds one zeroed control block per group.
+// Per-warp push buffers: 256 entries up to 512 threads per CTA (32 KB of
+// the CTA's static shared memory), 128 at 1024 threads.
+template <int BLOCK>
+constexpr unsigned kBatchQueueBuf = BLOCK <= 512 ? 256 : kQueueBuf;
+
 template <int BLOCK>
 __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK)
     batch_kernel(BatchJob *jobs, unsigned njobs, unsigned nbig, unsigned group, unsigned *cursors, char *scratch,
                  uint32_t hub_degree, TraversalCtl *gctl, unsigned long long timeout_ns)
 {
     __shared__ TraversalCtl s_ctl;
-    __shared__ uint32_t s_near[BLOCK / 32][kQueueBuf];
-    __shared__ uint32_t s_far[BLOCK / 32][kQueueBuf];
+    constexpr unsigned QB = kBatchQueueBuf<BLOCK>;
+    __shared__ uint32_t s_near[BLOCK / 32][QB];
+    __shared__ uint32_t s_far[BLOCK / 32][QB];
     __shared__ unsigned s_job;
     // The running job's parameters live in shared memory: the traversal
     // bodies read them by reference, which keeps them out of registers.
@@ -145,8 +151,8 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK)
             const unsigned long long t0 = s_t0;
             const unsigned tid = rank * BLOCK + threadIdx.x;
             GridMode m{gs, ctl, tid, group * BLOCK, tid / 32, group * BLOCK / 32};
-            if (s_app == 1) sssp_body(s_p, m, s_near[w], s_far[w]);
-            else bfs_body(s_p, m, s_near[w]);
+            if (s_app == 1) sssp_body<GridMode, false, QB>(s_p, m, s_near[w], s_far[w]);
+            else bfs_body<GridMode, false, QB>(s_p, m, s_near[w]);
             gs.epoch = m.gs.epoch;
             const bool ok = gs.sync();
             if (rank == 0 && threadIdx.x == 0) {
@@ -179,8 +185,8 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK)
         __syncthreads();
         const unsigned long long t0 = s_t0;
         CtaMode m{&s_ctl, threadIdx.x, BLOCK, w, BLOCK / 32, 0};
-        if (s_app == 1) sssp_body(s_p, m, s_near[w], s_far[w]);
-        else bfs_body(s_p, m, s_near[w]);
+        if (s_app == 1) sssp_body<CtaMode, false, QB>(s_p, m, s_near[w], s_far[w]);
+        else bfs_body<CtaMode, false, QB>(s_p, m, s_near[w]);
         __syncthreads();
         if (threadIdx.x == 0) write_result(jobs[j], s_ctl, t0);
         __syncthreads();

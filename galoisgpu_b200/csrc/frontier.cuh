@@ -98,7 +98,7 @@ __device__ __forceinline__ uint32_t ld_bits(const uint32_t *p)
         return __ldcg(p);
 }
 
-template <bool kLocalBits = false>
+template <bool kLocalBits = false, unsigned kQB = kQueueBuf>
 struct BfsVisitorT {
     static constexpr int kBatch = GFT_BFS_BATCH;  // edges per lane in one flattened step
     static constexpr bool kEarlyRow = false;      // owner() loads nothing
@@ -109,7 +109,7 @@ struct BfsVisitorT {
     int32_t *level;
     uint32_t *parent;
     int newlevel;
-    WarpQueue q;
+    WarpQueueT<kQB> q;  // pushes of the next frontier, a kQB-entry buffer per warp
     unsigned long long edges;  // per lane
     unsigned long long claimed;
     bool vec;
@@ -508,8 +508,8 @@ __device__ __forceinline__ unsigned pick_grain(unsigned n, unsigned nwarps, bool
 // the visited bitmap and own them for the level, so each sets its word's
 // new bits with one plain store; claimed vertices are also queued, so a
 // top-down level can follow.
-template <bool kLocalBits>
-__device__ __forceinline__ void bottom_up_level(BfsVisitorT<kLocalBits> &vis, const TravParams &p, unsigned L,
+template <bool kLocalBits, unsigned kQB>
+__device__ __forceinline__ void bottom_up_level(BfsVisitorT<kLocalBits, kQB> &vis, const TravParams &p, unsigned L,
                                                 unsigned gwarp, unsigned nwarps, unsigned lane)
 {
     const uint32_t n = p.nnodes, nwords = (n + 31) >> 5;
@@ -598,9 +598,11 @@ struct CtaMode {
 constexpr unsigned kAlpha = 14, kBeta = 24, kScan = 32;
 
 // kLocalBits: p.visited points to shared memory (one CTA runs the traversal).
-template <class Mode, bool kLocalBits = false>
+// warp_buf: this warp's kQB-entry push buffer.
+template <class Mode, bool kLocalBits = false, unsigned kQB = kQueueBuf>
 __device__ __forceinline__ void bfs_body(const TravParams &p, Mode &m, uint32_t *warp_buf)
 {
+    using Vis = BfsVisitorT<kLocalBits, kQB>;
     TraversalCtl *ctl = m.ctl;
     const unsigned lane = threadIdx.x & 31;
     const unsigned tid = m.tid, nthreads = m.nthreads, nwarps = m.nwarps, gwarp = m.gwarp;
@@ -622,7 +624,7 @@ __device__ __forceinline__ void bfs_body(const TravParams &p, Mode &m, uint32_t 
     }
     if (!m.sync()) return;
 
-    BfsVisitorT<kLocalBits> vis;
+    Vis vis;
     vis.edge_dst = p.edge_dst;
     // Skewed graphs sum the claimed vertices' out-degrees for the direction
     // switch; on uniform-degree graphs the frontier's size times the mean
@@ -656,7 +658,7 @@ __device__ __forceinline__ void bfs_body(const TravParams &p, Mode &m, uint32_t 
     // vertices: 16 per warp.)
     const unsigned min_grain =
         (kLocalBits && p.uniform)
-            ? max(1u, min(32u, 32u * BfsVisitorT<kLocalBits>::kBatch / max(1u, (unsigned)ceilf(mean_deg))))
+            ? max(1u, min(32u, 32u * Vis::kBatch / max(1u, (unsigned)ceilf(mean_deg))))
             : 1u;
     // The frontier's out-degree sum is only gathered on skewed graphs.
     const bool sum_degrees = p.dir_opt && !p.uniform;
@@ -711,8 +713,8 @@ __device__ __forceinline__ void bfs_body(const TravParams &p, Mode &m, uint32_t 
             bottom_up_level(vis, p, L, gwarp, nwarps, lane);
         } else {
             const unsigned grain = max(min_grain, pick_grain(n_in, nwarps, p.uniform));
-            expand_frontier<BfsVisitorT<kLocalBits>, BfsOwn>(vis, p, sel2(p.q, L), n_in, u32_of(ctl->claim[slot]),
-                                                             &ctl->hub[slot].v, grain, gwarp, nwarps, lane);
+            expand_frontier<Vis, BfsOwn>(vis, p, sel2(p.q, L), n_in, u32_of(ctl->claim[slot]), &ctl->hub[slot].v,
+                                         grain, gwarp, nwarps, lane);
         }
         vis.q.flush(lane);
         if (sum_degrees) {
@@ -722,8 +724,8 @@ __device__ __forceinline__ void bfs_body(const TravParams &p, Mode &m, uint32_t 
         if (!m.sync()) return;
         const unsigned long long hv = bottom_up ? 0ull : m.ld64(&ctl->hub[slot].v);
         if (hv) {
-            expand_hubs<BfsVisitorT<kLocalBits>, BfsOwn>(vis, p, (unsigned)(hv >> 32), (unsigned)hv,
-                                                         u32_of(ctl->hub_claim[slot]), gwarp, nwarps, lane);
+            expand_hubs<Vis, BfsOwn>(vis, p, (unsigned)(hv >> 32), (unsigned)hv, u32_of(ctl->hub_claim[slot]),
+                                     gwarp, nwarps, lane);
             vis.q.flush(lane);
             if (sum_degrees) {
                 warp_add_u32(mf_next, (unsigned)vis.mf, lane);

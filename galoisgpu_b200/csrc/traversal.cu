@@ -36,16 +36,20 @@ constexpr int kCtaBlock = 1024;  // threads of the single-CTA kernels
 // ---------------------------------------------------------------------------
 // Single-query kernels: the whole cooperative grid is one group.
 // ---------------------------------------------------------------------------
+// Push buffers of the grid-wide BFS kernel: 256 entries per warp (one
+// buffer per warp, at most 32 KB per CTA), as the grid-wide SSSP kernel.
+constexpr unsigned kBfsGridQueueBuf = 256;
+
 template <int BLOCK>
 __global__ void __launch_bounds__(BLOCK, 2048 / BLOCK) bfs_persistent(TravParams p)
 {
-    __shared__ uint32_t s_buf[BLOCK / 32][kQueueBuf];
+    __shared__ uint32_t s_buf[BLOCK / 32][kBfsGridQueueBuf];
     if ((int)blockIdx.x == p.skip_block) return;  // test hook: this CTA never arrives
     TraversalCtl *ctl = p.ctl;
     const unsigned tid = blockIdx.x * BLOCK + threadIdx.x, nthreads = gridDim.x * BLOCK;
     GridMode m{{&ctl->barrier.v, u32_of(ctl->release), &ctl->error, &ctl->error_where, gridDim.x, 0, p.timeout_ns},
                ctl, tid, nthreads, tid / 32, nthreads / 32};
-    bfs_body(p, m, s_buf[threadIdx.x >> 5]);
+    bfs_body<GridMode, false, kBfsGridQueueBuf>(p, m, s_buf[threadIdx.x >> 5]);
 }
 
 // Push buffers of the grid-wide SSSP kernel: 256 entries per warp up to 512
