@@ -89,7 +89,12 @@ typedef struct gft_tuning {
     int32_t test_skip_block;  /* test hook: CTA that never arrives (-1 = none)      */
     uint32_t max_blocks;      /* cap on the persistent grid; 0 = automatic (graphs
                                  of <= 2^17 vertices and <= 2^19 edges run on one
-                                 CTA, larger ones on the whole grid); 1 = one CTA */
+                                 CTA, larger ones on the whole grid); 1 = one CTA.
+                                 One CTA has 1024 threads whatever block_threads
+                                 says; BFS there on a graph of <= 2^17 vertices
+                                 and out-degrees <= 32 gives each thread a
+                                 frontier vertex and always runs top-down
+                                 (levels are the same either way) */
     uint32_t group_blocks;    /* batches: CTAs that share one large query (0 = 8)   */
     uint32_t group_min_nodes; /* batches: queries on graphs with at least this many
                                  vertices run on a CTA group (0 = 262144; set it
