@@ -347,6 +347,8 @@ def bench_workload(gft, name: str, steps: int, warmup: int, d, dev: int, headlin
         max_deg = int(np.diff(host.row_start.astype(np.int64)).max(initial=0))
         kname = ("sssp_single_cta" if app == "sssp" else
                  "bfs_cta_lanes" if dg.nnodes <= 1 << 17 and max_deg <= 32 else "bfs_single_cta")
+        tune_desc = {"launch": "one CTA of 1024 threads (graphs of <= 2^17 vertices and <= 2^19 edges)",
+                     "kernel": kname}
     traffic, traffic_src = profile_traffic(name, kname)
     res = {
         "name": name,
