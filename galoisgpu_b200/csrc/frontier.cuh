@@ -756,9 +756,11 @@ __device__ __forceinline__ void bfs_body(const TravParams &p, Mode &m, uint32_t 
 // distance decreases and claims.
 // Piles larger than this are not fused: every warp is busy with them
 // already, and chasing only lengthens the wait at the barrier (road
-// 4096^2: 3.88 ms fusing every pile, 3.66 ms up to 262144, 3.74 ms up to
-// 65536, 3.92 ms up to 16384).
-constexpr unsigned kFuseMaxPile = 262144;
+// 4096^2 with 128-entry push buffers: 3.88 ms fusing every pile, 3.66 ms
+// up to 262144, 3.74 ms up to 65536, 3.92 ms up to 16384; with 256-entry
+// buffers: 3.53 ms up to 524288, 3.57 ms up to 262144, 3.56 ms up to
+// 131072 or 1048576).
+constexpr unsigned kFuseMaxPile = 524288;
 
 __device__ __forceinline__ bool sssp_claim(unsigned long long *dt, uint32_t v, uint32_t near_tag)
 {

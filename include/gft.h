@@ -110,7 +110,7 @@ typedef struct gft_tuning {
                                  the iteration that found them (0 = engine
                                  default: 256 on graphs of uniform degree,
                                  never on skewed ones; UINT32_MAX = never;
-                                 near piles above 262144 vertices are never
+                                 near piles above 524288 vertices are never
                                  fused)                                       */
 } gft_tuning;
 
