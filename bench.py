@@ -26,17 +26,26 @@ one JSON line.
                against the measured HBM copy bandwidth
   cpu_baseline the CPU oracle (serial Dijkstra / FIFO BFS, one core) on the
                same query, rank 0 at N = 1 only; also checks bit-exact parity
+  reference_cuda  N = 1 only: the reference's own CUDA build for sm_100a
+               (oracle/_ref, built from the reference sources) on the same
+               graphs and sources in the same run: its kernel-only and
+               `Total time`, GTEPS, the ratio to this engine, and bit-exact
+               parity of every checked query against this engine's output
+               (the headline source, 16 RMAT-24 sources, the 256^2 grid);
+               --no-reference-build skips it
   secondary    N = 1 only: BFS on RMAT-24 (64 seeded sources, harmonic-mean
-               GTEPS) and on the 256^2 grid; 512 batched SSSP queries;
-               256-source BFS on RMAT-24; serving 8 resident graphs under
-               Poisson load; connected components, PageRank and maximal
-               independent set on RMAT-24 and the road grid (--workload
-               cc-rmat-24, pr-road-4096, mis-rmat-24, ... runs one alone)
+               GTEPS, all 64 checked against the CPU oracle) and on the 256^2
+               grid; 512 batched SSSP queries; 256-source BFS on RMAT-24;
+               serving 8 resident graphs under Poisson load; connected
+               components, PageRank and maximal independent set on RMAT-24
+               and the road grid (--workload cc-rmat-24, pr-road-4096,
+               mis-rmat-24, ... runs one alone)
 
---impl reference runs the reference arm: the reference has no CPU
-implementation of this path, so the oracle's restatement of it (kind
-"port") runs the same queries on all host threads (one query per thread per
-step); rank 0 only.
+--impl reference runs the reference arm: the reference's own CUDA build
+(oracle/_ref/{bfs,sssp}_multi) on the same seeded graph, sources and step
+count, timed on this GPU (the reference has no CPU implementation of this
+path).  It loads no part of this engine: the graph comes from
+oracle/libgrgen.so.  Rank 0 only.
 
 Multi-GPU: each rank is an independent replica (queries do not shard without
 a per-level exchange), so scaling is weak and no collective touches the data
@@ -50,9 +59,12 @@ import concurrent.futures as cf
 import json
 import math
 import os
+import re
+import shutil
 import statistics
 import subprocess
 import sys
+import tempfile
 import threading
 import time
 from pathlib import Path
@@ -374,12 +386,15 @@ def bench_workload(gft, name: str, steps: int, warmup: int, d, dev: int, headlin
                      "kernel": kname, "traffic_source": traffic_src},
         "clocks": clk,
         "graph_bytes": (dg.nnodes + 1) * 4 + dg.nedges * (8 if dg.weighted else 4),
+        "weighted": bool(dg.weighted),
         "tuning": tune_desc,
+        "tune": tune,
         "delta": delta,
         "query_stats": qstats[:4],
         "host": host,
         "out_last": out,
         "timed_src": timed_src,
+        "kms": kms,
         "reach": reach,
     }
     eng.close()
@@ -430,23 +445,13 @@ def our_arm(args) -> int:
         "vs_baseline": None,
         "dtype": "u32",
         "data": "synthetic: seeded graph generated on the device (SplitMix64 streams), same graph on every rank",
-        "config": {
-            "workload": name,
-            "app": spec["app"],
-            "graph": {k: v for k, v in spec.items() if k not in ("app", "nsrc", "src_seed", "delta")},
-            **({"reference_default_delta": spec["delta"]} if "delta" in spec else {}),
-            "nodes": res["nodes"],
-            "edges": res["edges"],
-            "sources": res["sources"],
-            "E_r_per_query": res["e_r_per_query"],
-            "V_r_per_query": res["v_r_per_query"],
-            "gteps_graph500": res["gteps_graph500"],
-            "l2": ("inputs larger than L2 (graph %.2f GB > 126 MB), no flush" % (res["graph_bytes"] / 1e9))
-            if res["graph_bytes"] > L2_BYTES else "graph smaller than L2 (resident between steps)",
-            "parallelism": f"replicas x{d.world}",
+        "config": workload_config(name, spec, res["nodes"], res["edges"], res["weighted"], res["timed_src"],
+                                  res["e_r_per_query"], res["v_r_per_query"], d.world),
+        "detail": {
             "kernel_ms_mean": res["kernel_ms_mean"],
             "gteps_hmean_kernel": res["gteps_hmean_kernel"],
-            "delta": res["delta"],
+            "gteps_graph500": res["gteps_graph500"],
+            **({"delta": res["delta"]} if spec["app"] == "sssp" else {}),
             "tuning": res["tuning"] or "engine defaults",
             "query_stats": res["query_stats"],
         },
@@ -468,6 +473,17 @@ def our_arm(args) -> int:
         cb, parity = cpu_baseline(orc, spec, res["host"], src, res["reach"], gpu_ref)
         line["cpu_baseline"] = cb
         line["parity"] = {"vs_oracle": parity, "source": src}
+        # The reference's own CUDA build on the same graph and source, in this run.
+        ref_blocks = {}
+        if not args.no_reference_build:
+            try:
+                ref_blocks[name] = reference_build_block(
+                    gft, name, spec, res["host"], dg, dev, [src], res["delta"], _kms_by_source(res), res["reach"],
+                    repeat=5, our_e2e_gteps=res["e2e"]["value"], tune=res["tune"])
+            except Exception as ex:
+                ref_blocks[name] = {"error": repr(ex)}
+            line["parity"]["vs_reference_build"] = ref_blocks[name].get("parity_vs_reference_build")
+            line["parity"]["sources_checked"] = {name: ref_blocks[name].get("sources_checked", 0)}
         if not args.no_secondary:
             sec = {}
             for sname in ("bfs-rmat-24", "bfs-grid-256"):
@@ -479,8 +495,9 @@ def our_arm(args) -> int:
                     r2, dg2 = bench_workload(gft, sname, 64 if sname == "bfs-rmat-24" else args.steps, 3, d, dev,
                                              headline=False)
                     s2 = r2["timed_src"][0]
-                    cb2, par2 = cpu_baseline(orc, WORKLOADS[sname], r2["host"], s2, r2["reach"],
-                                             _rerun(gft, dg2, WORKLOADS[sname], s2, dev))
+                    spec2 = WORKLOADS[sname]
+                    cb2, par2 = cpu_baseline(orc, spec2, r2["host"], s2, r2["reach"],
+                                             _rerun(gft, dg2, spec2, s2, dev))
                     sec[sname] = {
                         "tuning": r2["tuning"], "query_stats": r2["query_stats"][:2],
                         "value": r2["value"], "unit": "GTEPS", "gteps_hmean_kernel": r2["gteps_hmean_kernel"],
@@ -489,6 +506,21 @@ def our_arm(args) -> int:
                         "edges": r2["edges"], "E_r_per_query": r2["e_r_per_query"], "e2e": r2["e2e"],
                         "roofline": r2["roofline"], "cpu_baseline": cb2, "parity_vs_oracle": par2,
                     }
+                    srcs2 = sorted(set(r2["timed_src"]), key=r2["timed_src"].index)
+                    if len(srcs2) > 1:
+                        # Every timed source against the CPU oracle, on all host threads.
+                        sec[sname]["parity_vs_oracle_all_sources"] = oracle_parity_many(
+                            orc, spec2, r2["host"], _digests(gft, dg2, spec2, srcs2, dev, r2["tune"]),
+                            max(1, min(16, _cores())))
+                    if not args.no_reference_build:
+                        try:
+                            ref_blocks[sname] = reference_build_block(
+                                gft, sname, spec2, r2["host"], dg2, dev, srcs2[:16], None, _kms_by_source(r2),
+                                r2["reach"], repeat=2 if len(srcs2) > 1 else 5,
+                                our_e2e_gteps=r2["e2e"]["value"], tune=r2["tune"])
+                        except Exception as ex:
+                            ref_blocks[sname] = {"error": repr(ex)}
+                        line["parity"]["sources_checked"][sname] = ref_blocks[sname].get("sources_checked", 0)
                     dg2.free()
                 except Exception as ex:  # keep the headline line even if a secondary fails
                     sec[sname] = {"error": repr(ex)}
@@ -526,6 +558,8 @@ def our_arm(args) -> int:
                 except Exception as ex:
                     sec[cname] = {"error": repr(ex)}
             line["secondary"] = sec
+        if ref_blocks:
+            line["reference_cuda"] = ref_blocks
     if d.rank == 0:
         print(json.dumps(line), flush=True)
     d.barrier()
@@ -954,6 +988,40 @@ def bench_serve(gft, dev: int, rates=(100, 200, 400, 700, 1000, 1500, 2000, 3000
     }
 
 
+def _kms_by_source(res) -> dict:
+    """Median kernel time of each timed source of a bench_workload result."""
+    by: dict = {}
+    for s, km in zip(res["timed_src"], res["kms"]):
+        by.setdefault(s, []).append(km)
+    return {s: statistics.median(v) for s, v in by.items()}
+
+
+def _cores() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def _digests(gft, dg, spec, sources, dev, tune=None) -> dict:
+    """sha256 of this engine's result for every source."""
+    import hashlib
+
+    import torch
+
+    eng = gft.Engine(dev)
+    out = torch.empty(dg.nnodes, dtype=torch.int32, device=f"cuda:{dev}")
+    dig = {}
+    for s in sources:
+        if spec["app"] == "sssp":
+            eng.sssp(dg, s, delta=spec["delta"], out=out, tune=tune)
+        else:
+            eng.bfs(dg, s, out=out, tune=tune)
+        dig[s] = hashlib.sha256(out.cpu().numpy().tobytes()).hexdigest()
+    eng.close()
+    return dig
+
+
 def _rerun(gft, dg, spec, src, dev):
     eng = gft.Engine(dev)
     out = (eng.sssp(dg, src, delta=spec["delta"]) if spec["app"] == "sssp" else eng.bfs(dg, src))["out"]
@@ -962,81 +1030,270 @@ def _rerun(gft, dg, spec, src, dev):
 
 
 # ---------------------------------------------------------------------------
-# reference arm (CPU restatement, all host threads)
+# the reference's own CUDA build (oracle/_ref, compiled for sm_100a from the
+# reference sources by oracle/ref/Makefile)
 # ---------------------------------------------------------------------------
-def host_threads(spec, host) -> int:
-    """Usable host threads, capped so concurrent oracle queries fit in half
-    of the available memory (a Dijkstra query holds a heap of E entries)."""
+REF_BUILD = ROOT / "oracle" / "_ref"
+_REF_QUERY = re.compile(r"oracle-ref-query source (\d+) total_ns (\d+) kernel_ms ([0-9.]+)")
+
+
+def run_reference_build(app: str, gr_path, sources, delta=None, repeat: int = 1, dump_dir=None,
+                        timeout: float = 1200.0):
+    """Runs the reference's BFS or SSSP (its gg_main, kernels and worklists,
+    apps/bfs/kernel.cu:380-393, apps/sssp/kernel.cu:455-480) once per source
+    and repetition in one process (oracle/_ref/{bfs,sssp}_multi, see
+    oracle/ref/multi_driver.cu), the way skel.cu runs one query: the graph
+    read by the reference's own reader, `-d delta` for SSSP.  Returns one
+    dict per call in call order: source, total_ns (the reference's timer
+    around gg_main, skelapp/skel.cu:55-66, worklist allocations included)
+    and kernel_ms (CUDA events around every kernel the call launched)."""
+    exe = REF_BUILD / f"{app}_multi"
+    if not exe.exists():
+        raise FileNotFoundError(f"{exe} is not built (make -C oracle/ref)")
+    env = dict(os.environ, GFT_REF_SOURCES=",".join(str(int(x)) for x in sources), GFT_REF_REPEAT=str(repeat))
+    if dump_dir is not None:
+        env["GFT_REF_DUMP"] = str(dump_dir)
+    cmd = [str(exe), "-q", "-s", str(int(sources[0]))]
+    if app == "sssp":
+        cmd += ["-d", str(int(delta))]
+    cmd.append(str(gr_path))
+    r = subprocess.run(cmd, env=env, capture_output=True, text=True, timeout=timeout)
+    if r.returncode != 0:
+        raise RuntimeError(f"{exe.name} exited {r.returncode}: {r.stderr[-1500:]}")
+    calls = [{"source": int(m[1]), "total_ns": int(m[2]), "kernel_ms": float(m[3])}
+             for m in _REF_QUERY.finditer(r.stderr)]
+    if len(calls) != len(sources) * repeat:
+        raise RuntimeError(f"{exe.name}: {len(calls)} query lines for {len(sources) * repeat} calls")
+    return calls
+
+
+def _hmean(xs):
+    return len(xs) / sum(1.0 / x for x in xs) if xs else None
+
+
+def reference_build_block(gft, name: str, spec: dict, host, dg, dev: int, sources, our_delta, our_kms: dict,
+                          reach: dict, repeat: int, our_e2e_gteps=None, tune=None) -> dict:
+    """The reference's own sm_100a build on the same graph (written as .gr
+    and read by the reference's reader) and the same sources, in this run:
+    its kernel-only and `Total time`, GTEPS from the same E_r, the ratio to
+    this engine, and bit-exact parity of every query's result (its
+    node_data against this engine's output for the same source).  The
+    reference runs SSSP with its default delta (10000, apps/sssp/support.cu:10);
+    distances do not depend on delta.  Calls of
+    the first repetition are cold (the process's first gg_main also sets up
+    the drivers' barriers), so with repeat > 1 the times are the later
+    repetitions'."""
+    app = spec["app"]
+    tmp = Path(tempfile.mkdtemp(prefix="gft_refbuild_"))
     try:
-        cores = len(os.sched_getaffinity(0))
-    except AttributeError:
-        cores = os.cpu_count() or 1
-    per_query = (16 * host.nedges + 24 * host.nnodes) if spec["app"] == "sssp" else 8 * host.nnodes
-    try:
-        import psutil
+        gr = tmp / f"{name}.gr"
+        host.write(gr)
+        dump = tmp / "dump"
+        dump.mkdir()
+        t = time.time()
+        calls = run_reference_build(app, gr, sources, delta=spec.get("delta"), repeat=repeat, dump_dir=dump)
+        wall = time.time() - t
+        warm = calls[len(sources):] if repeat > 1 else calls
+        eng = gft.Engine(dev)
+        mismatches = []
+        import torch
 
-        avail = psutil.virtual_memory().available
-    except Exception:
-        avail = 8 << 30
-    return max(1, min(cores, int(avail * 0.5 // max(per_query, 1))))
+        out = torch.empty(dg.nnodes, dtype=torch.int32, device=f"cuda:{dev}")
+        for s in sources:
+            if app == "sssp":
+                eng.sssp(dg, s, delta=our_delta, out=out, tune=tune)
+            else:
+                eng.bfs(dg, s, out=out, tune=tune)
+            ref = np.fromfile(dump / f"{s}.i32", dtype=np.int32)
+            if ref.shape[0] != dg.nnodes or not np.array_equal(ref, out.cpu().numpy()):
+                mismatches.append(int(s))
+        eng.close()
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
+    by_src: dict = {}
+    for c in warm:
+        by_src.setdefault(c["source"], []).append(c)
+    ref_k = {s: statistics.median(x["kernel_ms"] for x in cs) for s, cs in by_src.items()}
+    ref_t = {s: statistics.median(x["total_ns"] for x in cs) / 1e6 for s, cs in by_src.items()}
+    e_r = {s: reach[s][1] for s in sources}
+    ref_gteps = _hmean([e_r[s] / (ref_k[s] * 1e6) for s in sources])
+    ref_total_gteps = _hmean([e_r[s] / (ref_t[s] * 1e6) for s in sources])
+    ours = _hmean([e_r[s] / (our_kms[s] * 1e6) for s in sources if s in our_kms])
+    res = {
+        "binary": f"oracle/_ref/{app}_multi (the reference's gg_main, kernels and worklists, compiled for sm_100a)",
+        "sources": len(sources),
+        "calls": len(calls),
+        "kernel_ms_mean": statistics.mean(ref_k.values()),
+        "total_ms_mean": statistics.mean(ref_t.values()),
+        "gteps_kernel": ref_gteps,
+        "gteps_total_time": ref_total_gteps,
+        "this_engine_gteps_kernel": ours,
+        "speedup_kernel": (ours / ref_gteps) if ours and ref_gteps else None,
+        "parity_vs_reference_build": "bit-exact" if not mismatches else f"{len(mismatches)} MISMATCHES {mismatches[:8]}",
+        "sources_checked": len(sources),
+        "process_wall_s": wall,
+        "note": "kernel_ms: CUDA events around every kernel of a gg_main call (init, worklist set-up, the persistent "
+                "driver); total_ms: the reference's own timer around gg_main, its worklist cudaMallocs included "
+                "(padded by the harness, oracle/ref/launch_wrap.cu); GTEPS as the harmonic mean over sources",
+    }
+    if our_e2e_gteps is not None and ref_total_gteps:
+        res["this_engine_e2e_gteps"] = our_e2e_gteps
+        res["speedup_e2e_vs_total_time"] = our_e2e_gteps / ref_total_gteps
+    log(f"[{name}] reference build: kernel {res['kernel_ms_mean']:.3f} ms ({ref_gteps:.2f} GTEPS), total "
+        f"{res['total_ms_mean']:.1f} ms; this engine {ours:.2f} GTEPS; parity {res['parity_vs_reference_build']}")
+    return res
 
-def reference_arm(args) -> int:
-    rank = int(os.environ.get("RANK", "0"))
-    if rank != 0:
-        return 0
-    import galoisgpu_b200 as gft
-    from oracle import oracle as orc
 
-    name = args.workload
-    spec = WORKLOADS[name]
-    host = make_host_graph(gft, spec)
-    sources = sources_for(spec, host)
-    threads = host_threads(spec, host)
-    reach = {}
-    for s in sources[:1]:
-        val = (orc.sssp(host.row_start, host.edge_dst, host.edge_data, s) if spec["app"] == "sssp"
-               else orc.bfs(host.row_start, host.edge_dst, s))
-        reach[s] = orc.reach_stats(host.row_start, val)
+def oracle_parity_many(orc, spec, host, gpu_digests: dict, threads: int) -> dict:
+    """Every source's result from this engine (as a digest) against the CPU
+    oracle's, the oracle queries spread over host threads."""
+    import hashlib
 
     def one(s):
         if spec["app"] == "sssp":
-            orc.sssp(host.row_start, host.edge_dst, host.edge_data, s)
+            ref = orc.sssp(host.row_start, host.edge_dst, host.edge_data, s)
         else:
-            orc.bfs(host.row_start, host.edge_dst, s)
+            ref = orc.bfs(host.row_start, host.edge_dst, s)
+        return s, hashlib.sha256(ref.tobytes()).hexdigest() == gpu_digests[s]
 
-    s0 = sources[0]
-    step_times = []
+    t = time.perf_counter()
     with cf.ThreadPoolExecutor(max_workers=threads) as ex:
-        for i in range(args.warmup + args.steps):
-            t = time.perf_counter()
-            list(ex.map(one, [s0] * threads))
-            if i >= args.warmup:
-                step_times.append(time.perf_counter() - t)
-    total = sum(step_times)
-    value = threads * reach[s0][1] * len(step_times) / total / 1e9
+        res = list(ex.map(one, list(gpu_digests)))
+    bad = [s for s, ok in res if not ok]
+    return {"sources_checked": len(res), "result": "bit-exact" if not bad else f"{len(bad)} MISMATCHES {bad[:8]}",
+            "threads": threads, "wall_s": time.perf_counter() - t}
+
+
+# ---------------------------------------------------------------------------
+# reference arm: the reference's own CUDA build on this GPU
+# ---------------------------------------------------------------------------
+def workload_config(name: str, spec: dict, nnodes: int, nedges: int, weighted: bool, timed_src, e_r: float,
+                    v_r: float, world: int) -> dict:
+    """The workload description both arms print (identical for the same
+    workload, graph and sources)."""
+    graph_bytes = (nnodes + 1) * 4 + nedges * (8 if weighted else 4)
+    return {
+        "workload": name,
+        "app": spec["app"],
+        "graph": {k: v for k, v in spec.items() if k not in ("app", "nsrc", "src_seed", "delta")},
+        **({"reference_default_delta": spec["delta"]} if "delta" in spec else {}),
+        "nodes": nnodes,
+        "edges": nedges,
+        "sources": list(timed_src) if len(timed_src) <= 4 else f"{len(set(timed_src))} seeded (seed {spec['src_seed']})",
+        "E_r_per_query": e_r,
+        "V_r_per_query": v_r,
+        "l2": ("inputs larger than L2 (graph %.2f GB > 126 MB), no flush" % (graph_bytes / 1e9))
+        if graph_bytes > L2_BYTES else "graph smaller than L2 (resident between steps)",
+        "parallelism": f"replicas x{world}",
+    }
+
+
+def _visible_gpu() -> str:
+    v = os.environ.get("CUDA_VISIBLE_DEVICES", "").split(",")[0].strip()
+    return v or "0"
+
+
+def reference_arm(args) -> int:
+    """The reference's own BFS/SSSP, compiled for sm_100a from its sources
+    (oracle/_ref, oracle/ref/Makefile), on the same seeded graph, sources and
+    step count as the engine's arm.  The graph comes from oracle/libgrgen.so
+    (the engine's generators built without the engine library) and is
+    written as .gr for the reference's own reader.  One process runs the
+    reference's gg_main once per step (oracle/ref/multi_driver.cu): `value`
+    is E_r over the summed device time of each call's kernels, `e2e` E_r
+    over the reference's own timer around gg_main (its worklist allocations
+    included).  Rank 0 only; other ranks exit at once."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    name = args.workload
+    spec = WORKLOADS.get(name)
+    exe = REF_BUILD / f"{spec['app']}_multi" if spec else None
+    if spec is None or not exe.exists():
+        why = (f"no reference build for workload {name}" if spec is None else
+               f"{exe.relative_to(ROOT)} is not built (make -C oracle/ref needs the reference sources)")
+        print(json.dumps({"impl": "reference", "unavailable": why}), flush=True)
+        return 0
+    from oracle import grgen
+    from oracle import oracle as orc
+
+    kw = {k: v for k, v in spec.items() if k not in ("kind", "seed", "app", "nsrc", "src_seed", "delta")}
+    if spec["kind"] == "grid":
+        kw["max_weight"] = 1
+    t0 = time.time()
+    host = grgen.generate(spec["kind"], spec["seed"], **kw)
+    sources = [0] if spec["nsrc"] == 0 else host.pick_sources(spec["src_seed"], spec["nsrc"])
+    step_src = [sources[i % len(sources)] for i in range(max(args.steps, len(sources)))]
+    timed_src = step_src[:args.steps] if len(sources) <= args.steps else sources
+    warm_src = [sources[i % len(sources)] for i in range(args.warmup)]
+    distinct = sorted(set(timed_src), key=timed_src.index)
+    tmp = Path(tempfile.mkdtemp(prefix="gft_refarm_"))
+    try:
+        gr = tmp / f"{name}.gr"
+        host.write_gr(gr)
+        log(f"[reference] {name}: graph {host.nnodes} nodes {host.nedges} edges written in {time.time() - t0:.1f}s")
+        dump = tmp / "dump"
+        dump.mkdir()
+        # First pass: one call per distinct source, results dumped for E_r.
+        first = run_reference_build(spec["app"], gr, distinct, delta=spec.get("delta"), dump_dir=dump)
+        reach = {}
+        for s in distinct:
+            val = np.fromfile(dump / f"{s}.i32", dtype=np.int32)
+            reach[s] = orc.reach_stats(host.row_start, val)
+        clocks = ClockSampler(_visible_gpu())
+        calls = run_reference_build(spec["app"], gr, warm_src + list(timed_src), delta=spec.get("delta"))
+        clk = clocks.stop()
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
+    timed = calls[len(warm_src):]
+    kms = [c["kernel_ms"] for c in timed]
+    tot = [c["total_ns"] / 1e6 for c in timed]
+    e_sum = sum(reach[c["source"]][1] for c in timed)
+    v_sum = sum(reach[c["source"]][0] for c in timed)
+    k = len(timed)
+    value = e_sum / (sum(kms) * 1e6)
+    e2e_value = e_sum / (sum(tot) * 1e6)
+    per_q = [reach[c["source"]][1] / (c["kernel_ms"] * 1e6) for c in timed]
     line = {
         "impl": "reference",
         "metric": "GTEPS per query",
         "value": value,
         "unit": "GTEPS",
         "n_gpus": args.gpus,
-        "steps": args.steps,
+        "steps": k,
         "warmup": args.warmup,
-        "ms_per_step": total / len(step_times) * 1e3,
+        "ms_per_step": statistics.mean(kms),
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
         "dtype": "u32",
-        "data": "synthetic: same seeded graph as the gft arm, generated on the host",
-        "config": {"workload": name, "app": spec["app"], "nodes": host.nnodes, "edges": host.nedges,
-                   "sources": [s0], "E_r_per_query": reach[s0][1]},
-        "cpu_baseline": {"value": value, "unit": "GTEPS", "cores": threads, "kind": "port",
-                         "sample": f"{threads} concurrent {spec['app'].upper()} queries from source {s0} per step "
-                                   "(the reference has no CPU implementation of this path; this is the oracle's "
-                                   "restatement of its semantics)"},
-        "e2e": {"value": value, "unit": "GTEPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "data": "synthetic: the same seeded graph and sources as the gft arm (oracle/libgrgen.so), written as .gr and "
+                "read by the reference's own reader",
+        "config": workload_config(name, spec, host.nnodes, host.nedges, host.edge_data is not None, timed_src,
+                                  e_sum / k, v_sum / k, 1),
+        "detail": {
+            "binary": f"oracle/_ref/{spec['app']}_multi: the reference's gg_main, kernels and worklists "
+                      "(apps/{bfs,sssp}/kernel.cu) compiled for sm_100a; one process, one gg_main call per step",
+            **({"delta": spec["delta"]} if spec["app"] == "sssp" else {}),
+            "kernel_ms_mean": statistics.mean(kms),
+            "total_time_ms_mean": statistics.mean(tot),
+            "gteps_hmean_kernel": len(per_q) / sum(1.0 / x for x in per_q),
+            "launch": "the reference's own sizing: kernel_sizing (8 CTAs of 256 per SM), persistent driver at "
+                      "min(blocks, SMs x residency), launched cooperatively by the harness",
+        },
+        "e2e": {"value": e2e_value, "unit": "GTEPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0,
+                "note": "E_r over the reference's own timer around gg_main (skelapp/skel.cu:55-66): its worklist "
+                        "cudaMallocs, init kernels and the traversal; the graph is already on the device and the "
+                        "result stays there, as in the reference's CLI"},
+        "cpu_baseline": {"value": value, "unit": "GTEPS", "cores": 1, "kind": "reference",
+                         "sample": f"{k} {spec['app'].upper()} queries of the reference's own CUDA build on this "
+                                   "B200 (the reference has no CPU implementation of this path), driven by one host "
+                                   "thread"},
+        "gpu_launches": None,
+        "clocks": clk,
     }
     print(json.dumps(line), flush=True)
+    host.close()
     return 0
 
 
@@ -1051,6 +1308,8 @@ def main(argv=None) -> int:
                     default=HEADLINE, help="a traversal workload (the headline by default), or a connected-components, "
                                            "PageRank or maximal-independent-set one")
     ap.add_argument("--no-secondary", action="store_true", help="skip the secondary workloads")
+    ap.add_argument("--no-reference-build", action="store_true",
+                    help="skip running the reference's own CUDA build (oracle/_ref) beside this engine")
     args = ap.parse_args(argv)
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")

@@ -289,8 +289,10 @@ struct gft_batch {
     gft::TraversalCtl *d_gctl = nullptr;
     size_t gctl_bytes = 0;
     std::vector<uint32_t> order;      // job slot -> caller's query index
-    gft::BatchJob *h_jobs = nullptr;  // pinned
+    gft::BatchJob *h_jobs = nullptr;  // pinned, caller-owned inputs: the graph's first node uploads it
+    gft::BatchJob *h_res = nullptr;   // pinned, the job table as the last launch left it
     gft::BatchJob *d_jobs = nullptr;
+    bool in_flight = false;           // submitted and not yet waited for
     unsigned *d_cursor = nullptr;
     char *d_scratch = nullptr;
     size_t scratch_bytes = 0;
@@ -316,6 +318,7 @@ void gft_batch_destroy(gft_batch *b)
     if (b->ev0) cudaEventDestroy(b->ev0);
     if (b->ev1) cudaEventDestroy(b->ev1);
     if (b->h_jobs) cudaFreeHost(b->h_jobs);
+    if (b->h_res) cudaFreeHost(b->h_res);
     if (b->d_jobs) cudaFree(b->d_jobs);
     if (b->d_cursor) cudaFree(b->d_cursor);
     if (b->d_scratch) cudaFree(b->d_scratch);
@@ -364,6 +367,7 @@ gft_status gft_batch_create(gft_engine *e, const gft_query *q, uint32_t n, const
     DeviceScope device_scope(e->device);
     cudaError_t err = device_scope.err;
     if (err == cudaSuccess) err = cudaMallocHost(&b->h_jobs, sizeof(BatchJob) * n);
+    if (err == cudaSuccess) err = cudaMallocHost(&b->h_res, sizeof(BatchJob) * n);
     if (err != cudaSuccess) {
         gft_batch_destroy(b);
         return fail(GFT_ERR_OOM, "gft_batch_create: %s", cudaGetErrorString(err));
@@ -423,6 +427,9 @@ gft_status gft_batch_create(gft_engine *e, const gft_query *q, uint32_t n, const
 gft_status gft_batch_set_source(gft_batch *b, uint32_t query, uint32_t src)
 {
     if (!b || query >= b->n) return fail(GFT_ERR_INVALID_ARG, "gft_batch_set_source: bad batch or index");
+    // The replay uploads h_jobs when its first node runs, which may be after
+    // submit returns: changing it before the wait could reach the running batch.
+    if (b->in_flight) return fail(GFT_ERR_BUSY, "gft_batch_set_source: a submit is in flight; call gft_batch_wait first");
     for (uint32_t s = 0; s < b->n; s++)
         if (b->order[s] == query) {
             if (src >= b->h_jobs[s].nnodes) return fail(GFT_ERR_INVALID_ARG, "gft_batch_set_source: source out of range");
@@ -440,6 +447,7 @@ gft_status gft_batch_submit(gft_batch *b, void *stream)
     cudaStream_t s = (cudaStream_t)stream;
     GFT_CUDA_TRY(cudaEventRecord(b->ev0, s));
     GFT_CUDA_TRY(cudaGraphLaunch(b->exec, s));
+    b->in_flight = true;
     GFT_CUDA_TRY(cudaEventRecord(b->ev1, s));
     b->last_stream = s;
     return GFT_OK;
@@ -451,13 +459,14 @@ gft_status gft_batch_wait(gft_batch *b, gft_query *q, gft_batch_stats *st)
     DeviceScope device_scope(b->engine->device);
     GFT_CUDA_TRY(device_scope.err);
     cudaStream_t s = b->last_stream;
-    GFT_CUDA_TRY(cudaMemcpyAsync(b->h_jobs, b->d_jobs, sizeof(BatchJob) * b->n, cudaMemcpyDeviceToHost, s));
+    GFT_CUDA_TRY(cudaMemcpyAsync(b->h_res, b->d_jobs, sizeof(BatchJob) * b->n, cudaMemcpyDeviceToHost, s));
     GFT_CUDA_TRY(cudaStreamSynchronize(s));
+    b->in_flight = false;
     gft_status worst = GFT_OK;
     unsigned long long t_first = ~0ull, t_last = 0;
     uint64_t edges = 0;
     for (uint32_t k = 0; k < b->n; k++) {
-        const BatchJob &j = b->h_jobs[k];
+        const BatchJob &j = b->h_res[k];
         if (j.status && worst == GFT_OK) worst = (gft_status)j.status;
         t_first = std::min(t_first, j.t_start);
         t_last = std::max(t_last, j.t_end);

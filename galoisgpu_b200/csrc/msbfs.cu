@@ -481,6 +481,13 @@ gft_status gft_msbfs_levels(const uint32_t *d_planes, uint32_t nnodes, uint32_t 
                             int32_t *d_out, void *stream)
 {
     if (!d_planes || !d_out || i >= k || k > 256) return fail(GFT_ERR_INVALID_ARG, "gft_msbfs_levels: bad argument");
+    // Launch on the device that holds the planes, whatever device is current.
+    cudaPointerAttributes attr;
+    GFT_CUDA_TRY(cudaPointerGetAttributes(&attr, d_planes));
+    if (attr.type != cudaMemoryTypeDevice && attr.type != cudaMemoryTypeManaged)
+        return fail(GFT_ERR_INVALID_ARG, "gft_msbfs_levels: d_planes is not device memory");
+    DeviceScope device_scope(attr.device);
+    GFT_CUDA_TRY(device_scope.err);
     dev::msbfs_levels_kernel<<<1184, 256, 0, (cudaStream_t)stream>>>(d_planes, nnodes, row_words(k), levels, i, d_out);
     GFT_CUDA_TRY(cudaGetLastError());
     return GFT_OK;

@@ -786,6 +786,12 @@ extern "C" gft_status gft_bfs_noalloc(const gft_graph *g, uint32_t src, int32_t 
     p.timeout_ns = (unsigned long long)timeout_ms * 1000000ull;
     p.skip_block = -1;
     p.vec_ok = ((uintptr_t)G.edge_dst % 16 == 0);
+    // The same schedule choices as gft_bfs: static chunks on uniform-degree
+    // graphs, bottom-up levels on a graph marked symmetric (they use only the
+    // bitmap and queues above).
+    p.nedges = G.nedges;
+    p.uniform = G.max_degree <= kUniformDegree;
+    p.dir_opt = G.symmetric && !(tune && tune->direction != 0);
 
     // The control block must start at zero for every call.
     GFT_CUDA_TRY(cudaMemsetAsync(p.ctl, 0, sizeof(TraversalCtl), stream));

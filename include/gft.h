@@ -271,7 +271,9 @@ GFT_API gft_status gft_sssp_host_many(gft_engine *e, const gft_graph *g, const u
  * (about 16.2 MB, held by every GPU that loads libgft until exit), so the
  * graph may have at most 1,048,576 vertices; larger graphs are rejected with
  * GFT_ERR_INVALID_ARG.  The caller passes the graph and the output buffers
- * (d_level, optional d_parent) as for gft_bfs; results are identical.
+ * (d_level, optional d_parent) as for gft_bfs; results are identical, and
+ * the schedule is gft_bfs's too (bottom-up levels on a graph marked
+ * symmetric unless tune->direction says otherwise).
  * The first call on a device looks up the array's device address
  * (cudaGetSymbolAddress with that device current); make that first call
  * before any stream capture.  Every call reuses the same array (the control
@@ -323,7 +325,9 @@ typedef struct gft_batch gft_batch;
  * launch.  tune: block_threads (256/512/1024), blocks_per_sm, hub_degree. */
 GFT_API gft_status gft_batch_create(gft_engine *e, const gft_query *q, uint32_t n, const gft_tuning *tune,
                                     gft_batch **out);
-/* Changes query `query`'s source for the next submit (no re-capture). */
+/* Changes query `query`'s source for the next submit (no re-capture).
+ * Returns GFT_ERR_BUSY between a submit and its gft_batch_wait: the replay
+ * reads the job table when it starts on the device. */
 GFT_API gft_status gft_batch_set_source(gft_batch *b, uint32_t query, uint32_t src);
 /* Replays the captured launch on `stream` (asynchronous). */
 GFT_API gft_status gft_batch_submit(gft_batch *b, void *stream);
@@ -409,7 +413,10 @@ GFT_API gft_status gft_serve_close(gft_server *s);
  * has one row of WP words per vertex, WP = ceil(k / 32) rounded up to 1, 2,
  * 4 or 8; in plane L, bit i % 32 of word i / 32 of vertex v's row is set iff
  * source i reaches v at level L.  stats->levels = planes used;
- * GFT_ERR_OVERFLOW if the traversal needs more than max_levels.
+ * GFT_ERR_OVERFLOW if the traversal needs more than max_levels.  The last
+ * level is only known to be last once its expansion found nothing new, which
+ * needs room for one more plane: give max_levels >= levels + 1 (a graph whose
+ * sources reach everything within D hops needs D + 2).
  * gft_msbfs_levels writes source i's int32 levels (as gft_bfs would) from
  * the planes.  flags: GFT_MSBFS_SYMMETRIC allows bottom-up levels (the
  * graph's out-edges must also be its in-edges); without it every level is

@@ -3,10 +3,24 @@ mix of concurrent requests equals the same query run alone (bit for bit),
 requests really are batched and overlapped, and admission errors are
 statuses."""
 
+import time
+
 import numpy as np
 import pytest
 
 pytestmark = pytest.mark.gpu
+
+
+def drain(srv, n: int, deadline_s: float = 120.0) -> dict:
+    """Polls until n completions arrived; fails (instead of waiting forever)
+    when one is lost."""
+    got = {}
+    t_end = time.monotonic() + deadline_s
+    while len(got) < n:
+        assert time.monotonic() < t_end, f"only {len(got)} of {n} completions within {deadline_s} s"
+        for c in srv.poll(256, 100000):
+            got[c["ticket"]] = c
+    return got
 
 
 def test_mix_equals_alone(gft, engine):
@@ -28,10 +42,7 @@ def test_mix_equals_alone(gft, engine):
         out = torch.full((devs[gi].nnodes,), -5, dtype=torch.int32, device="cuda")
         t = srv.enqueue(devs[gi], app, src, out, delta=[100, 40000][i % 2])
         reqs.append((t, gi, app, src, out, [100, 40000][i % 2]))
-    got = {}
-    while len(got) < len(reqs):
-        for c in srv.poll(256, 100000):
-            got[c["ticket"]] = c
+    got = drain(srv, len(reqs))
     st = srv.stats()
     srv.close()
     assert all(c["status"] == 0 for c in got.values())
@@ -53,9 +64,7 @@ def test_idle_server_gives_a_heavy_request_the_device(gft, engine):
     srv = Server(engine, group_min_nodes=1 << 12, group_blocks=8, lane_arena_bytes=64 << 20)
     out = torch.empty(d.nnodes, dtype=torch.int32, device="cuda")
     srv.enqueue(d, "sssp", 3, out, delta=1000)
-    got = []
-    while not got:
-        got = srv.poll(4, 100000)
+    got = list(drain(srv, 1).values())
     srv.close()
     assert got[0]["status"] == 0 and got[0]["width"] > 1
     np.testing.assert_array_equal(out.cpu().numpy(), engine.sssp(d, 3, delta=1000)["out"].cpu().numpy())
@@ -114,10 +123,7 @@ def test_wide_pool_for_skewed_sssp(gft, engine):
         src = host.pick_sources(500 + i, 1)[0]
         out = torch.full((devs[gi].nnodes,), -5, dtype=torch.int32, device="cuda")
         reqs.append((srv.enqueue(devs[gi], app, src, out, delta=300), gi, app, src, out))
-    got = {}
-    while len(got) < len(reqs):
-        for c in srv.poll(256, 100000):
-            got[c["ticket"]] = c
+    got = drain(srv, len(reqs))
     srv.close()
     wide = [got[t] for t, gi, app, _, _ in reqs if gi == 0 and app == "sssp"]
     assert wide and all(c["lane"] == 1 and c["width"] >= 2 for c in wide)
