@@ -17,7 +17,10 @@ from .graph import (  # noqa: F401
     Engine,
     Tune,
     output,
+    output_gz,
     reach_stats,
+    read_node_data,
+    write_node_data,
     write_cc_output,
     write_pr_output,
     write_mis_output,

@@ -168,6 +168,12 @@ _SIGS: dict[str, tuple] = {
     "gft_last_error": (C.c_char_p, []),
     "gft_status_string": (C.c_char_p, [C.c_int]),
     "gft_gr_read": (C.c_int, [C.c_char_p, C.POINTER(Csr)]),
+    "gft_gr_read_chunked": (C.c_int, [C.c_char_p, C.POINTER(Csr)]),
+    "gft_graph_load_gr": (C.c_int, [C.c_int, C.c_char_p, _P, C.POINTER(_P)]),
+    "gft_ingest_release": (None, []),
+    "gft_write_output_gz": (C.c_int, [C.c_char_p, C.c_uint32, _P, C.c_int]),
+    "gft_write_node_data": (C.c_int, [C.c_char_p, C.c_uint32, _P, C.c_uint32]),
+    "gft_read_node_data": (C.c_int, [C.c_char_p, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), _P]),
     "gft_gr_write": (C.c_int, [C.c_char_p, C.POINTER(Csr)]),
     "gft_csr_free": (None, [C.POINTER(Csr)]),
     "gft_gen_grid": (C.c_int, [C.c_uint32, C.c_uint32, C.c_uint64, C.c_uint32, C.POINTER(Csr)]),

@@ -33,6 +33,8 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 LIB_SOURCES = [
     "graph_io.cpp",
+    "ingest.cpp",
+    "output.cpp",
     "gen_host.cpp",
     "engine.cu",
     "traversal.cu",
@@ -120,7 +122,7 @@ def build(force: bool = False, verbose: bool = False, ptxas_verbose: bool = Fals
             f.result()
     if force or todo or _newer(LIB, objs):
         tmp = LIB.with_suffix(".so.tmp")
-        _run([NVCC, *ARCH, "-shared", "-cudart", "static", "-o", str(tmp), *map(str, objs), "-lpthread"], verbose)
+        _run([NVCC, *ARCH, "-shared", "-cudart", "static", "-o", str(tmp), *map(str, objs), "-lpthread", "-lz"], verbose)
         os.replace(tmp, LIB)
     cli_src = CSRC / CLI_SOURCE
     if cli_src.exists():

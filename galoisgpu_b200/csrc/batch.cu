@@ -60,9 +60,8 @@ __device__ __forceinline__ TravParams job_params(const BatchJob &jb, char *scrat
     if (jb.app == 1) {
         p.far[0] = reinterpret_cast<uint32_t *>(base + 2 * qbytes);
         p.far[1] = reinterpret_cast<uint32_t *>(base + 3 * qbytes);
-        p.far_stamp = reinterpret_cast<uint32_t *>(base + 4 * qbytes);
-        p.dt = reinterpret_cast<unsigned long long *>(base + 5 * qbytes);
-        p.hubs = reinterpret_cast<uint2 *>(base + 7 * qbytes);
+        p.qstamp = reinterpret_cast<uint32_t *>(base + 4 * qbytes);
+        p.hubs = reinterpret_cast<uint2 *>(base + 5 * qbytes);
     } else {
         const size_t vbytes = ((size_t)((jb.nnodes + 31) / 32) * 4 + 255) & ~(size_t)255;
         p.parent = jb.parent;
@@ -270,7 +269,7 @@ size_t batch_job_scratch(uint32_t app, uint32_t nnodes, uint32_t hub_cap)
 {
     const size_t qbytes = ((size_t)nnodes * 4 + 255) & ~(size_t)255;
     const size_t hbytes = ((size_t)hub_cap * 8 + 255) & ~(size_t)255;
-    if (app == 1) return 7 * qbytes + hbytes;  // 4 queues, far stamps, 8-byte (dist, tag) words
+    if (app == 1) return 5 * qbytes + hbytes;  // 4 queues, pile stamps (distances in place in `out`)
     const size_t vbytes = ((size_t)((nnodes + 31) / 32) * 4 + 255) & ~(size_t)255;
     return 2 * qbytes + vbytes + hbytes;
 }

@@ -19,6 +19,12 @@
 // accepted for compatibility; this engine always balances per vertex inside
 // its persistent kernel.  Errors are reported and turned into a non-zero
 // exit code instead of exit(1) deep inside the library.
+//
+// Two additions for large results and graphs: `-b file` writes the result
+// array as a binary dump (gft_write_node_data), and an -o file name ending
+// in ".gz" gets the same text gzip-compressed (gft_write_output_gz; bfs and
+// sssp).  Every app but cc reads the .gr file straight into device memory
+// (gft_graph_load_gr); cc's output lists every edge, so it keeps a host copy.
 #include <getopt.h>
 #include <stdint.h>
 #include <stdio.h>
@@ -50,8 +56,8 @@ static const char *kAppArgsUsage =
 
 static void usage(const char *argv0)
 {
-    fprintf(stderr, "usage: %s [-q] [-g gpunum] [-o output-file] %s graph-file \n %s\n", argv0, kAppUsage,
-            kAppArgsUsage);
+    fprintf(stderr, "usage: %s [-q] [-g gpunum] [-o output-file] [-b binary-dump] %s graph-file \n %s\n", argv0,
+            kAppUsage, kAppArgsUsage);
 }
 
 static uint64_t now_ns()
@@ -75,14 +81,15 @@ int main(int argc, char **argv)
     }
     int quiet = 0, device = 0, start_node = 0, delta = 10000, no_print_rank = 0;
     uint32_t max_iterations = 0xFFFFFFFFu;
-    const char *output = nullptr;
+    const char *output = nullptr, *dump = nullptr;
     char opts[32];
-    snprintf(opts, sizeof opts, "g:qo:%s", kAppOpts);
+    snprintf(opts, sizeof opts, "g:qo:b:%s", kAppOpts);
     int c;
     while ((c = getopt(argc, argv, opts)) != -1) {
         switch (c) {
         case 'q': quiet = 1; break;
         case 'o': output = optarg; break;
+        case 'b': dump = optarg; break;
         case 'g': {
             char *end;
             device = (int)strtol(optarg, &end, 10);
@@ -124,19 +131,27 @@ int main(int argc, char **argv)
             : GFT_CLI_PR ? "persistent residual-push PageRank" : GFT_CLI_CC ? "union-find CC"
             : GFT_CLI_SSSP ? "persistent near-far SSSP" : "persistent BFS");
     gft_csr h;
+    memset(&h, 0, sizeof h);
+    gft_graph *g = nullptr;
+    gft_engine *e = nullptr;
     uint64_t t0 = now_ns();
-    gft_status s = gft_gr_read(input, &h);
-    if (s != GFT_OK) return die("read", s);
+    gft_status s;
+    if (GFT_CLI_CC) {
+        if ((s = gft_gr_read(input, &h)) != GFT_OK) return die("read", s);
+        if ((s = gft_graph_upload(device, &h, nullptr, &g)) != GFT_OK) return die("upload", s);
+    } else {
+        if ((s = gft_graph_load_gr(device, input, nullptr, &g)) != GFT_OK) return die("read", s);
+        int weighted = 0;
+        gft_graph_info(g, &h.nnodes, &h.nedges, &weighted);
+    }
     printf("nnodes=%u, nedges=%u.\n", h.nnodes, h.nedges);
     printf("read %s in %llu ms\n", input, (unsigned long long)((now_ns() - t0) / 1000000));
     if (!GFT_CLI_NO_SOURCE && (uint32_t)start_node >= h.nnodes) {
         fprintf(stderr, "start node %d out of range (%u nodes)\n", start_node, h.nnodes);
+        gft_graph_free(g);
         gft_csr_free(&h);
         return EXIT_FAILURE;
     }
-    gft_graph *g = nullptr;
-    gft_engine *e = nullptr;
-    if ((s = gft_graph_upload(device, &h, nullptr, &g)) != GFT_OK) return die("upload", s);
     if ((s = gft_engine_create(device, &e)) != GFT_OK) return die("engine", s);
     printf("Using GPU: %d\n", device);
 
@@ -195,9 +210,16 @@ int main(int argc, char **argv)
         } else if (GFT_CLI_CC) {
             s = gft_write_cc_output(output, &h, val.data());
         } else {
-            s = gft_write_output(output, h.nnodes, val.data());
+            const size_t len = strlen(output);
+            s = len > 3 && strcmp(output + len - 3, ".gz") == 0 ? gft_write_output_gz(output, h.nnodes, val.data(), 1)
+                                                                : gft_write_output(output, h.nnodes, val.data());
         }
         if (s != GFT_OK) rc = die("output", s);
+    }
+    if (!quiet && dump) {
+        s = GFT_CLI_PR ? gft_write_node_data(dump, h.nnodes, rank.data(), GFT_ELEM_F32)
+                       : gft_write_node_data(dump, h.nnodes, val.data(), GFT_ELEM_I32);
+        if (s != GFT_OK) rc = die("binary dump", s);
     }
     gft_engine_destroy(e);
     gft_graph_free(g);

@@ -53,6 +53,16 @@ __global__ void max_degree_kernel(const uint32_t *__restrict__ row_start, uint32
     if ((threadIdx.x & 31) == 0 && m) atomicMax(out, m);
 }
 
+// Lowest index of an edge whose destination is >= n, into *first.
+__global__ void first_bad_edge(const uint32_t *__restrict__ dst, uint32_t m, uint32_t n, unsigned long long *first)
+{
+    for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < m; e += gridDim.x * blockDim.x)
+        if (__ldcs(dst + e) >= n) {
+            atomicMin(first, (unsigned long long)e);
+            return;
+        }
+}
+
 __global__ void interleave_edges(const uint32_t *__restrict__ dst, const int32_t *__restrict__ w, uint32_t m,
                                  uint2 *__restrict__ out)
 {
@@ -100,6 +110,25 @@ gft_status graph_degree_stats(DeviceGraph &G, cudaStream_t stream)
     if (err == cudaSuccess) err = cudaStreamSynchronize(stream);
     GFT_CUDA_TRY(err);
     G.max_degree = h;
+    return GFT_OK;
+}
+
+gft_status check_edges_device(const DeviceGraph &G, cudaStream_t stream, uint64_t *first_bad)
+{
+    unsigned long long *d = nullptr, h = ~0ull;
+    *first_bad = ~0ull;
+    if (!G.nedges) return GFT_OK;
+    GFT_CUDA_TRY(cudaMallocAsync(&d, sizeof h, stream));
+    cudaError_t err = cudaMemcpyAsync(d, &h, sizeof h, cudaMemcpyHostToDevice, stream);
+    if (err == cudaSuccess) {
+        dev::first_bad_edge<<<148 * 8, 256, 0, stream>>>(G.edge_dst, G.nedges, G.nnodes, d);
+        err = cudaGetLastError();
+    }
+    if (err == cudaSuccess) err = cudaMemcpyAsync(&h, d, sizeof h, cudaMemcpyDeviceToHost, stream);
+    cudaFreeAsync(d, stream);
+    if (err == cudaSuccess) err = cudaStreamSynchronize(stream);
+    GFT_CUDA_TRY(err);
+    *first_bad = h;
     return GFT_OK;
 }
 

@@ -38,8 +38,8 @@ struct TravParams {
     uint32_t *visited;  // BFS bitmap
     uint32_t *q[2];     // frontier / near pile
     uint32_t *far[2];   // SSSP far pile
-    unsigned long long *dt;  // SSSP: (dist << 32) | tag per vertex
-    uint32_t *far_stamp;
+    uint32_t *qstamp;   // SSSP: the last pile stamp per vertex (see SsspVisitorT); distances live in `out`
+    uint32_t *fused;    // SSSP bucket fusion: the distance a fused vertex was expanded at (kSolo), or NULL
     uint2 *hubs;
     uint32_t hub_cap;
     uint32_t hub_degree;
@@ -114,6 +114,7 @@ struct BfsVisitorT {
     unsigned long long claimed;
     bool vec;
 
+    __device__ __forceinline__ uint32_t vertex(uint32_t x) const { return x; }
     __device__ __forceinline__ BfsOwn owner(bool has, uint32_t u) const { return BfsOwn{u}; }
     __device__ __forceinline__ bool active(const BfsOwn &) const { return true; }
     __device__ __forceinline__ BfsOwn shfl(const BfsOwn &o, int lane) const
@@ -183,19 +184,35 @@ struct SsspOwn {
     uint32_t du;
 };
 
-// SSSP relaxation on a packed word per vertex, (dist << 32) | tag.  One
-// 64-bit atomicMin both lowers the distance and records who lowered it: an
-// improvement that leaves the vertex at or under the bucket threshold writes
-// this iteration's odd near tag, and it queues the vertex only if the tag it
-// replaced differs, so the near pile holds each vertex at most once per
-// iteration without a separate stamp array or a second atomic.  An
-// improvement above the threshold writes near_tag - 1 and is deduplicated in
-// the far pile with a per-phase stamp.
+// A near-pile entry with this bit set names a vertex that bucket fusion
+// already expanded in the iteration that queued it, at the distance it
+// recorded in p.fused (fusion is off on graphs of 2^31 vertices or more).
+constexpr uint32_t kFusedMark = 0x80000000u;
+
+// SSSP relaxation (apps/sssp/kernel.cu:244-259): nd = dist[u] + w; if nd
+// beats dist[v], atomicMin.  Distances are the 4-byte int32 output array
+// itself (a probe fetches a sector of eight of them, and the whole array
+// stays L2-resident on graphs of up to ~2^24 vertices).  An improvement then
+// stamps v in one 4-byte array with atomicMax, stamps increasing with the
+// iteration I: near (bucket threshold met) ((I + 1) << 1) | 1, far (I + 1)
+// << 1.
+//   - near: v joins the near pile unless the stamp it replaced is this
+//     iteration's near stamp (so the pile holds v at most once per
+//     iteration);
+//   - far: v joins the far pile unless the stamp it replaced is from the
+//     current phase (at or after phase_stamp), which the far split also
+//     writes for the vertices it carries over.
+// With atomicMax a far stamp can never replace a near stamp of the same
+// iteration: a far improvement that loses the race to a near one is then
+// correctly dropped (v's distance is already below the threshold), and a
+// later near improvement still finds the near stamp.  Once v is near in a
+// phase it cannot go far again in that phase (distances only fall), so a
+// near stamp hides no far-pile entry.
 //
 // kSolo: the single-query kernel's visitor, which also reads interleaved
-// (dst, weight) pairs when the graph has them and loads a vertex's row
-// alongside its distance; the batched kernel's jobs use the leaner
-// visitor, which keeps that kernel's register budget.
+// (dst, weight) pairs when the graph has them, loads a vertex's row
+// alongside its distance, and runs bucket fusion; the batched kernel's jobs
+// use the leaner visitor, which keeps that kernel's register budget.
 template <bool kSolo, unsigned kQB = kQueueBuf>
 struct SsspVisitorT {
     static constexpr int kBatch = GFT_SSSP_BATCH;  // edges per lane in one flattened step
@@ -204,19 +221,34 @@ struct SsspVisitorT {
     const uint32_t *__restrict__ edge_dst;
     const int32_t *__restrict__ edge_data;
     const uint2 *__restrict__ edge_dw;  // interleaved (dst, weight), or NULL
-    unsigned long long *dt;
-    uint32_t *far_stamp;
-    uint32_t near_tag, far_tag;
+    uint32_t *dist;
+    uint32_t *qstamp;
+    uint32_t *fused;                    // kFuse: distances at which fused vertices were expanded
+    uint32_t near_stamp, far_stamp, phase_stamp;
+    bool fusing;                        // kFuse: owner() records the distance it hands out
     unsigned long long threshold;
-    WarpQueueT<kQB> nq, fq;  // near and far pushes, kQB-entry buffers per warp
+    WarpQueueT<kQB, kFuse> nq;          // near pushes (with the fused entries' upper region)
+    WarpQueueT<kQB> fq;                 // far pushes; kQB-entry buffers per warp
     unsigned far_min;
     unsigned long long edges;
     unsigned *err, *err_where;
     bool vec;
 
-    __device__ __forceinline__ SsspOwn owner(bool has, uint32_t u) const
+    // The vertex of pile entry x (fused entries carry kFusedMark).
+    __device__ __forceinline__ uint32_t vertex(uint32_t x) const { return kFuse ? (x & ~kFusedMark) : x; }
+
+    // Owner of pile entry x: its distance, or INF (inactive) for a fused
+    // entry whose distance has not fallen since fusion expanded it.
+    __device__ __forceinline__ SsspOwn owner(bool has, uint32_t x) const
     {
-        return SsspOwn{u, has ? (uint32_t)(__ldcg(dt + u) >> 32) : kInf};
+        const uint32_t u = vertex(x);
+        if (!has) return SsspOwn{u, kInf};
+        const uint32_t du = __ldcg(dist + u);
+        if (kFuse) {
+            if ((x & kFusedMark) && __ldcg(fused + u) == du) return SsspOwn{u, kInf};
+            if (fusing) fused[u] = du;
+        }
+        return SsspOwn{u, du};
     }
     __device__ __forceinline__ bool active(const SsspOwn &o) const { return o.du != kInf; }
     __device__ __forceinline__ SsspOwn shfl(const SsspOwn &o, int lane) const
@@ -225,56 +257,46 @@ struct SsspVisitorT {
     }
 
     // K relaxations per lane, staged so that the lane's K distance probes,
-    // then its K atomicMins, then its far-pile stamps, are each in flight
-    // together: one memory latency per stage instead of one per edge.  Two of
-    // a lane's K edges may name the same vertex; its atomics then apply in
-    // program order, so the second one sees the first one's word and the
-    // vertex is queued once, as with one edge at a time.
+    // then its K atomicMins, then its K stamps, are each in flight together:
+    // one memory latency per stage instead of one per edge.  Two of a lane's
+    // K edges may name the same vertex; its atomics then apply in program
+    // order, so the second sees the first and the vertex is queued once, as
+    // with one edge at a time.
     template <int K>
     __device__ __forceinline__ void relaxK(const bool (&valid)[K], const uint32_t (&v)[K], const uint32_t (&w)[K],
                                            const SsspOwn (&o)[K], unsigned lane)
     {
-        unsigned long long cur[K];
-#ifdef GFT_NO_PRECHECK
+        uint32_t cur[K];
 #pragma unroll
-        for (int k = 0; k < K; k++) cur[k] = ~0ull;
-#else
-#pragma unroll
-        for (int k = 0; k < K; k++) cur[k] = valid[k] ? __ldcg(dt + v[k]) : 0ull;
-#endif
+        for (int k = 0; k < K; k++) cur[k] = valid[k] ? __ldcg(dist + v[k]) : 0u;
         uint32_t nd[K];
-        bool to_near[K], to_far[K];
+        bool imp[K], near[K];
 #pragma unroll
         for (int k = 0; k < K; k++) {
-            to_near[k] = to_far[k] = false;
+            imp[k] = near[k] = false;
             nd[k] = o[k].du + w[k];  // du < 2^31 and w < 2^32: a wrap is caught below
             if (!valid[k]) continue;
             edges++;
             if (nd[k] >= kInf || nd[k] < o[k].du) {
                 raise_error(err, err_where, GFT_ERR_OVERFLOW, o[k].u);
-            } else if (nd[k] < (uint32_t)(cur[k] >> 32)) {
-                const bool near = nd[k] <= threshold;
-                const unsigned long long mine = ((unsigned long long)nd[k] << 32) | (near ? near_tag : near_tag - 1);
-                cur[k] = atomicMin(dt + v[k], mine);
-                if (nd[k] < (uint32_t)(cur[k] >> 32)) {
-                    to_near[k] = near && (uint32_t)cur[k] != near_tag;
-                    to_far[k] = !near;
-                }
+            } else if (nd[k] < cur[k]) {
+                imp[k] = nd[k] < atomicMin(dist + v[k], nd[k]);
+                near[k] = nd[k] <= threshold;
             }
         }
-        uint32_t stamp[K];
+        uint32_t old[K];
 #pragma unroll
         for (int k = 0; k < K; k++) {
-            stamp[k] = far_tag;
-            if (to_far[k]) {
-                far_min = min(far_min, nd[k]);
-                stamp[k] = atomicExch(far_stamp + v[k], far_tag);
+            old[k] = 0;
+            if (imp[k]) {
+                if (!near[k]) far_min = min(far_min, nd[k]);
+                old[k] = atomicMax(qstamp + v[k], near[k] ? near_stamp : far_stamp);
             }
         }
 #pragma unroll
         for (int k = 0; k < K; k++) {
-            nq.push(to_near[k], v[k], lane);
-            fq.push(to_far[k] && stamp[k] != far_tag, v[k], lane);
+            nq.push(imp[k] && near[k] && old[k] != near_stamp, v[k], lane);
+            fq.push(imp[k] && !near[k] && old[k] < phase_stamp, v[k], lane);
         }
     }
     template <int K>
@@ -409,22 +431,25 @@ __device__ __forceinline__ void expand_lanes(Vis &vis, const TravParams &p, bool
     // A visitor whose owner() loads per-vertex state (the SSSP distance, the
     // PageRank residual) has the row loaded alongside it, not after it: both
     // depend only on u, so the loads share one memory round trip.
+    // u is a queue entry; vis.vertex(u) is its vertex (SSSP entries may
+    // carry a mark that owner() reads).
+    const uint32_t v = vis.vertex(u);
     uint32_t start = 0, deg = 0;
     if (Vis::kEarlyRow && has) {
-        start = __ldg(p.row_start + u);
-        deg = __ldg(p.row_start + u + 1) - start;
+        start = __ldg(p.row_start + v);
+        deg = __ldg(p.row_start + v + 1) - start;
     }
     Own o = vis.owner(has, u);
     if (!Vis::kEarlyRow && has && vis.active(o)) {
-        start = __ldg(p.row_start + u);
-        deg = __ldg(p.row_start + u + 1) - start;
+        start = __ldg(p.row_start + v);
+        deg = __ldg(p.row_start + v + 1) - start;
     }
     if (!(has && vis.active(o))) deg = 0;
     if (deg >= p.hub_degree) {
         unsigned nch = (deg + kHubChunk - 1) / kHubChunk;
         unsigned long long old = atomicAdd(hub_ctr, (1ull << 32) | nch);
         unsigned h = (unsigned)(old >> 32);
-        if (h < p.hub_cap) p.hubs[h] = make_uint2(u, (unsigned)old);
+        if (h < p.hub_cap) p.hubs[h] = make_uint2(v, (unsigned)old);
         else raise_error(&p.ctl->error, &p.ctl->error_where, GFT_ERR_OVERFLOW, h);
         deg = 0;
     }
@@ -746,14 +771,13 @@ __device__ __forceinline__ void bfs_body(const TravParams &p, Mode &m, uint32_t 
 // ---------------------------------------------------------------------------
 // SSSP body (near-far)
 // ---------------------------------------------------------------------------
-// Bucket fusion: a warp that pushed v to the near pile in this iteration may
-// expand v itself before the barrier.  It first claims v by swapping v's
-// tag from this iteration's near tag to another value, so that a later
-// improvement of v in the same iteration queues it again (the near-pile
-// test compares against the near tag); it then reads v's distance as the
-// expansion's owner, so no improvement is lost.  False when another warp's
-// claim changed the tag first.  The loop ends: the word only changes by
-// distance decreases and claims.
+// Bucket fusion (as in GraphIt's delta-stepping, Zhang et al., CGO 2020): a
+// warp that pushed v to the near pile in this iteration may expand v itself
+// before the barrier.  v stays in the pile, marked kFusedMark, and owner()
+// records in p.fused the distance the expansion used.  In the next
+// iteration the marked entry is skipped if v's distance is still that one,
+// and expanded again if an improvement came after.  Every read of p.fused
+// follows the write behind a barrier, so no claim protocol is needed.
 // Piles larger than this are not fused: every warp is busy with them
 // already, and chasing only lengthens the wait at the barrier (road
 // 4096^2 with 128-entry push buffers: 3.88 ms fusing every pile, 3.66 ms
@@ -762,22 +786,16 @@ __device__ __forceinline__ void bfs_body(const TravParams &p, Mode &m, uint32_t 
 // 131072 or 1048576).
 constexpr unsigned kFuseMaxPile = 524288;
 
-__device__ __forceinline__ bool sssp_claim(unsigned long long *dt, uint32_t v, uint32_t near_tag)
-{
-    unsigned long long w = __ldcg(dt + v);
-    while ((uint32_t)w == near_tag) {
-        const unsigned long long old = atomicCAS(dt + v, w, (w & 0xFFFFFFFF00000000ull) | (near_tag - 1));
-        if (old == w) return true;
-        w = old;
-    }
-    return false;
-}
-
-// Near-far loop state: bucket threshold (inclusive), iteration, phase.
+// Near-far loop state: bucket threshold (inclusive), iteration, phase, and
+// the iteration that started the phase.
 struct SsspState {
     unsigned long long T;
-    unsigned I, P;
+    unsigned I, P, Ps;
 };
+
+// Pile stamps (see SsspVisitorT): increasing with the iteration, never 0.
+__device__ __forceinline__ uint32_t near_stamp_of(unsigned I) { return ((I + 1u) << 1) | 1u; }
+__device__ __forceinline__ uint32_t far_stamp_of(unsigned I) { return (I + 1u) << 1; }
 
 // Is the coming iteration small enough for one CTA?  A near pile of at most
 // p.cta_small vertices, or a far split (empty near pile) of a far pile that
@@ -816,19 +834,21 @@ __device__ __forceinline__ int sssp_iter(const TravParams &p, Mode &m, Vis &vis,
     if (n_near > 0) {
         // Relax the near pile (apps/sssp/kernel.cu:177-306).
         vis.threshold = T;
-        vis.near_tag = 2 * I + 3;  // odd, distinct per iteration, never the initial 0
-        vis.far_tag = P + 1;
+        vis.near_stamp = near_stamp_of(I);
+        vis.far_stamp = far_stamp_of(I);
+        vis.phase_stamp = far_stamp_of(st.Ps);
         vis.far_min = kInf;
         vis.fq.queue = sel2(p.far, P);
         vis.fq.len = u32_of(ctl->far_len[P % 3]);
         expand_frontier<Vis, SsspOwn>(vis, p, sel2(p.q, I), n_near, u32_of(ctl->claim[slot]),
                                               &ctl->hub[slot].v, pick_grain(n_near, nwarps, p.uniform), gwarp, nwarps,
                                               lane);
-        if (Vis::kFuse && p.fuse && n_near <= kFuseMaxPile) {
-            // Bucket fusion (as in GraphIt's delta-stepping, Zhang et al.,
-            // CGO 2020): expand up to p.fuse of this warp's fresh near
+        if constexpr (Vis::kFuse) {
+            // Bucket fusion: expand up to p.fuse of this warp's fresh near
             // vertices now, newest first, instead of in the next iteration.
-            unsigned budget = p.fuse;
+            // They move to the buffer's upper region, marked, and still go
+            // to the pile.
+            unsigned budget = n_near <= kFuseMaxPile ? p.fuse : 0u;
             while (vis.nq.count && budget) {
                 const unsigned take = min(32u, vis.nq.count);
                 const unsigned base = vis.nq.count - take;
@@ -837,8 +857,10 @@ __device__ __forceinline__ int sssp_iter(const TravParams &p, Mode &m, Vis &vis,
                 __syncwarp();
                 vis.nq.count = base;
                 budget = budget > take ? budget - take : 0;
-                const bool mine = lane < take && sssp_claim(p.dt, v, vis.near_tag);
-                expand_lanes<Vis, SsspOwn>(vis, p, mine, v, &ctl->hub[slot].v, lane);
+                vis.nq.push_top(lane < take, v | kFusedMark, lane);
+                vis.fusing = true;
+                expand_lanes<Vis, SsspOwn>(vis, p, lane < take, v, &ctl->hub[slot].v, lane);
+                vis.fusing = false;
             }
         }
         vis.nq.flush(lane);
@@ -859,6 +881,8 @@ __device__ __forceinline__ int sssp_iter(const TravParams &p, Mode &m, Vis &vis,
         }
     } else {
         // Near pile drained: split the far pile with the next threshold.
+        // This iteration starts phase P + 1; the vertices carried over to
+        // its far pile get its phase stamp.
         const unsigned nf = m.ld(u32_of(ctl->far_len[P % 3]));
         if (nf == 0) return 1;
         const unsigned fmin = m.ld(u32_of(ctl->far_min[P % 3]));
@@ -872,6 +896,7 @@ __device__ __forceinline__ int sssp_iter(const TravParams &p, Mode &m, Vis &vis,
         }
         vis.fq.queue = sel2(p.far, (P + 1));
         vis.fq.len = u32_of(ctl->far_len[(P + 1) % 3]);
+        const uint32_t carry = far_stamp_of(I);
         const uint32_t *pile = sel2(p.far, P);
         unsigned local_min = kInf;
         const unsigned sgrain = pick_grain(nf, nwarps, p.uniform);
@@ -885,13 +910,13 @@ __device__ __forceinline__ int sssp_iter(const TravParams &p, Mode &m, Vis &vis,
                 unsigned d = kInf;
                 if (idx < end) {
                     v = __ldcg(pile + idx);
-                    d = (uint32_t)(__ldcg(p.dt + v) >> 32);
+                    d = __ldcg(vis.dist + v);
                 }
                 const bool live = idx < end && d > T_old;
                 const bool to_near = live && d <= T_new;
                 const bool to_far = live && d > T_new;
                 if (to_far) {
-                    p.far_stamp[v] = P + 2;
+                    p.qstamp[v] = carry;
                     local_min = min(local_min, d);
                 }
                 vis.nq.push(to_near, v, lane);
@@ -905,6 +930,7 @@ __device__ __forceinline__ int sssp_iter(const TravParams &p, Mode &m, Vis &vis,
         if (!m.sync()) return -1;
         st.T = T_new;
         st.P = P + 1;
+        st.Ps = I;
     }
     st.I = I + 1;
     return 0;
@@ -912,8 +938,8 @@ __device__ __forceinline__ int sssp_iter(const TravParams &p, Mode &m, Vis &vis,
 
 // kSolo: a single query (the persistent grid or the single-CTA kernel):
 // runs of small iterations may go to the first CTA of a grid launch (needs
-// p.cta_small), and the visitor reads interleaved edges.  The batched
-// kernel's jobs use the lean body.
+// p.cta_small), and the visitor reads interleaved edges and fuses buckets.
+// The batched kernel's jobs use the lean body.
 // near_buf and far_buf: this warp's kQB-entry push buffers.
 template <class Mode, bool kSolo = false, unsigned kQB = kQueueBuf>
 __device__ __forceinline__ void sssp_body(const TravParams &p, Mode &m, uint32_t *near_buf, uint32_t *far_buf)
@@ -921,13 +947,14 @@ __device__ __forceinline__ void sssp_body(const TravParams &p, Mode &m, uint32_t
     TraversalCtl *ctl = m.ctl;
     const unsigned lane = threadIdx.x & 31;
     const unsigned tid = m.tid, nthreads = m.nthreads, nwarps = m.nwarps, gwarp = m.gwarp;
-    unsigned long long *dt = p.dt;
+    uint32_t *dist = reinterpret_cast<uint32_t *>(p.out);
 
-    // Initialise (apps/sssp/kernel.cu:23-35): 0 at src, INF elsewhere.
+    // Initialise (apps/sssp/kernel.cu:23-35): 0 at src, INF elsewhere; the
+    // distances are computed in place in the output array.
     const uint32_t n = p.nnodes;
     for (uint32_t v = tid; v < n; v += nthreads) {
-        dt[v] = v == p.src ? 0ull : ((unsigned long long)kInf << 32);
-        p.far_stamp[v] = 0;
+        dist[v] = v == p.src ? 0u : kInf;
+        p.qstamp[v] = 0;
     }
     if (tid == 0) {
         p.q[0][0] = p.src;
@@ -940,21 +967,28 @@ __device__ __forceinline__ void sssp_body(const TravParams &p, Mode &m, uint32_t
     vis.edge_dst = p.edge_dst;
     vis.edge_data = p.edge_data;
     vis.edge_dw = p.edge_dw;
-    vis.dt = dt;
-    vis.far_stamp = p.far_stamp;
+    vis.dist = dist;
+    vis.qstamp = p.qstamp;
+    vis.fused = p.fused;
+    vis.fusing = false;
     vis.edges = 0;
     vis.err = &ctl->error;
     vis.err_where = &ctl->error_where;
     vis.vec = p.vec_ok;
     vis.nq.buf = near_buf;
     vis.nq.count = 0;
+    vis.nq.top = kQB;
     vis.nq.cap = p.qcap;
     vis.nq.err = &ctl->error;
     vis.nq.err_where = &ctl->error_where;
-    vis.fq = vis.nq;
     vis.fq.buf = far_buf;
+    vis.fq.count = 0;
+    vis.fq.top = kQB;
+    vis.fq.cap = p.qcap;
+    vis.fq.err = &ctl->error;
+    vis.fq.err_where = &ctl->error_where;
 
-    SsspState st{p.delta, 0, 0};
+    SsspState st{p.delta, 0, 0, 0};
     for (;;) {
         const unsigned n_near = m.ld(u32_of(ctl->qlen[st.I % 3]));
         if (kSolo && Mode::kGrid && p.cta_small && sssp_small(p, m, st, n_near)) {
@@ -973,6 +1007,7 @@ __device__ __forceinline__ void sssp_body(const TravParams &p, Mode &m, uint32_t
                 if (threadIdx.x == 0) {
                     ctl->handoff[0].v = st.T;
                     ctl->handoff[1].v = ((unsigned long long)(r > 0) << 63) | ((unsigned long long)st.P << 32) | st.I;
+                    ctl->handoff[2].v = st.Ps;
                 }
             }
             if (!m.sync()) return;
@@ -980,6 +1015,7 @@ __device__ __forceinline__ void sssp_body(const TravParams &p, Mode &m, uint32_t
             st.T = m.ld64(&ctl->handoff[0].v);
             st.I = (unsigned)h1;
             st.P = (unsigned)(h1 >> 32) & 0x7FFFFFFFu;
+            st.Ps = (unsigned)m.ld64(&ctl->handoff[2].v);
             if (h1 >> 63) break;
             continue;
         }
@@ -987,16 +1023,13 @@ __device__ __forceinline__ void sssp_body(const TravParams &p, Mode &m, uint32_t
         if (r < 0) return;
         if (r > 0) break;
     }
-    const unsigned long long T = st.T;
-    const unsigned P = st.P;
     // Every CTA leaves the loop after the same barrier, so all relaxations are
-    // done: write the int32 distances.
-    for (uint32_t v = tid; v < n; v += nthreads) p.out[v] = (int32_t)(uint32_t)(__ldcg(dt + v) >> 32);
+    // done and the output array holds the distances.
     warp_add_u64(&ctl->edges, vis.edges, lane);
     if (tid == 0) {
-        ctl->levels = P;
+        ctl->levels = st.P;
         ctl->iterations = m.epoch();
-        ctl->threshold = (unsigned)min(T, 0xFFFFFFFFull);
+        ctl->threshold = (unsigned)min(st.T, 0xFFFFFFFFull);
     }
 }
 

@@ -79,8 +79,9 @@ struct TraversalCtl {
     CtlLine far_len[3];    // SSSP far pile length per phase slot (u32)
     CtlLine far_min[3];    // SSSP least distance sent to the far pile per phase slot (u32)
     CtlLine job;           // batch kernel: job claimed by a CTA group (u32)
-    CtlLine handoff[2];    // SSSP: loop state left by the CTA that ran small iterations alone
-                           // ([0] threshold; [1] done << 63 | phase << 32 | iteration)
+    CtlLine handoff[3];    // SSSP: loop state left by the CTA that ran small iterations alone
+                           // ([0] threshold; [1] done << 63 | phase << 32 | iteration;
+                           // [2] the iteration that started the phase)
     // Cold fields, written once per launch.
     unsigned error;        // gft_status recorded by the device (0 = none)
     unsigned error_where;  // barrier episode or queue index of the failure
@@ -176,6 +177,8 @@ struct DeviceScope {
 // is being captured, the graph keeps the separate arrays only.
 gft_status ensure_edge_pairs(gft_graph *g, cudaStream_t stream);
 gft_status graph_degree_stats(DeviceGraph &G, cudaStream_t stream);
+// Index of the first edge whose destination is >= nnodes (~0 if none).
+gft_status check_edges_device(const DeviceGraph &G, cudaStream_t stream, uint64_t *first_bad);
 // Graphs whose out-degrees are all at most this many edges have near-equal
 // work per frontier vertex, so a frontier is split into one static chunk
 // per warp (no shared claim cursor); others are claimed dynamically.

@@ -122,6 +122,14 @@ class CSRGraph:
         check(load().gft_gr_read(str(path).encode(), C.byref(csr)))
         return cls(*_take_csr(csr))
 
+    @classmethod
+    def read_chunked(cls, path: str | Path) -> "CSRGraph":
+        """The same parse through the parallel chunked reader that
+        DeviceGraph.load_gr uses, into host arrays."""
+        csr = Csr()
+        check(load().gft_gr_read_chunked(str(path).encode(), C.byref(csr)))
+        return cls(*_take_csr(csr))
+
     def write(self, path: str | Path) -> None:
         c = self._csr()
         check(load().gft_gr_write(str(path).encode(), C.byref(c)))
@@ -213,6 +221,15 @@ class DeviceGraph:
             raise ValueError(f"unknown graph kind {kind!r}")
         h = C.c_void_p()
         check(load().gft_graph_generate(device, C.byref(p), _stream_ptr(stream), C.byref(h)))
+        return cls(h, device)
+
+    @classmethod
+    def load_gr(cls, path: str | Path, device: int = 0, stream=None) -> "DeviceGraph":
+        """Reads a .gr file straight into device memory (parallel chunked
+        reads into pinned staging, overlapped with the copies); replaces
+        CSRGraph::read + copy_to_gpu (rt/src/csr_graph.cu:152-261)."""
+        h = C.c_void_p()
+        check(load().gft_graph_load_gr(device, str(path).encode(), _stream_ptr(stream), C.byref(h)))
         return cls(h, device)
 
     @property
@@ -582,6 +599,33 @@ def output(path: str | Path, values: np.ndarray) -> None:
     check(load().gft_write_output(str(path).encode(), len(v), C.c_void_p(v.ctypes.data)))
 
 
+def output_gz(path: str | Path, values: np.ndarray, level: int = 1) -> None:
+    """The text of :func:`output`, gzip-compressed in parallel blocks (one
+    gzip member per 2^20 lines; readable as one stream by any gzip reader)."""
+    v = np.ascontiguousarray(values, dtype=np.int32)
+    check(load().gft_write_output_gz(str(path).encode(), len(v), C.c_void_p(v.ctypes.data), level))
+
+
+def write_node_data(path: str | Path, values: np.ndarray) -> None:
+    """Binary dump of a result array (int32 levels/distances/labels/states,
+    or float32 ranks) behind a 24-byte header."""
+    v = np.ascontiguousarray(values)
+    if v.dtype == np.float32:
+        kind = 1
+    else:
+        v, kind = np.ascontiguousarray(v, dtype=np.int32), 0
+    check(load().gft_write_node_data(str(path).encode(), len(v), C.c_void_p(v.ctypes.data), kind))
+
+
+def read_node_data(path: str | Path) -> np.ndarray:
+    """Reads a dump written by :func:`write_node_data` (or the CLI's -b)."""
+    n, kind = C.c_uint32(), C.c_uint32()
+    check(load().gft_read_node_data(str(path).encode(), C.byref(n), C.byref(kind), None))
+    out = np.empty(n.value, dtype=np.float32 if kind.value == 1 else np.int32)
+    check(load().gft_read_node_data(str(path).encode(), C.byref(n), C.byref(kind), C.c_void_p(out.ctypes.data)))
+    return out
+
+
 def write_cc_output(path: str | Path, graph: CSRGraph, labels: np.ndarray) -> None:
     """CC labels in the reference's format: a node line and one line per
     out-edge (apps/cc/support.cu:16-36)."""
@@ -615,6 +659,9 @@ __all__ = [
     "DEFAULT_DELTA",
     "reach_stats",
     "output",
+    "output_gz",
+    "write_node_data",
+    "read_node_data",
     "write_cc_output",
     "write_pr_output",
     "write_mis_output",

@@ -134,6 +134,12 @@ GFT_API const char *gft_status_string(gft_status s);
  * GFT_ERR_FORMAT.  Arrays are malloc'd; release with gft_csr_free.
  * ------------------------------------------------------------------------- */
 GFT_API gft_status gft_gr_read(const char *path, gft_csr *out);
+/* The same parse as gft_gr_read through the parallel chunked reader that
+ * gft_graph_load_gr uses (pread of 8 MB chunks by up to 8 threads, end
+ * offsets narrowed and checked per chunk), into host arrays: the host side
+ * of that pipeline, for checking it without a GPU.  Same results and
+ * errors as gft_gr_read. */
+GFT_API gft_status gft_gr_read_chunked(const char *path, gft_csr *out);
 GFT_API gft_status gft_gr_write(const char *path, const gft_csr *g);
 GFT_API void gft_csr_free(gft_csr *g);
 
@@ -169,6 +175,17 @@ GFT_API gft_status gft_pick_sources(const gft_csr *g, uint64_t seed, uint32_t k,
  * caller keeps them alive until gft_graph_free.
  * ------------------------------------------------------------------------- */
 GFT_API gft_status gft_graph_upload(int device, const gft_csr *g, void *stream, gft_graph **out);
+/* .gr file straight to the device: replaces CSRGraph::read + copy_to_gpu
+ * (rt/src/csr_graph.cu:152-261, a serial per-edge parse loop, then four
+ * synchronous pageable copies).  Worker threads pread 8 MB chunks into
+ * pinned staging buffers and copy each with cudaMemcpyAsync on their own
+ * stream while reading the next, so file reads and PCIe transfers overlap;
+ * end offsets are narrowed to u32 and checked on the host per chunk,
+ * destinations are checked on the device.  No host copy of the graph is
+ * made.  The pinned staging (128 MB) is allocated by the first call and kept
+ * for later ones until gft_ingest_release.  Errors as gft_gr_read. */
+GFT_API gft_status gft_graph_load_gr(int device, const char *path, void *stream, gft_graph **out);
+GFT_API void gft_ingest_release(void);
 GFT_API gft_status gft_graph_wrap(int device, uint32_t nnodes, uint32_t nedges, const uint32_t *d_row_start,
                           const uint32_t *d_edge_dst, const int32_t *d_edge_data, gft_graph **out);
 /* Generates a synthetic graph directly in device memory (same result as the
@@ -497,6 +514,27 @@ GFT_API gft_status gft_reach_stats(const gft_graph *g, const int32_t *d_val, voi
  * per node (apps/bfs/support.cu:27-45, apps/sssp/support.cu:34-53).
  * path "-" writes to stdout. */
 GFT_API gft_status gft_write_output(const char *path, uint32_t nnodes, const int32_t *h_val);
+
+/* Output path for large results (no counterpart in the reference, whose
+ * output() formats every line with one fprintf, apps/sssp/support.cu:34-53;
+ * the text of a 16.8 M-vertex result is ~250 MB).
+ * gft_write_output_gz: the same text as gft_write_output, gzip-compressed
+ * (zlib `level` 1..9, 0 = 1).  Blocks of 2^20 lines are formatted and
+ * deflated on all host threads, each block a complete gzip member; members
+ * are written in order, so the file is one valid gzip stream (RFC 1952
+ * allows concatenated members) that gunzip, zcat or zlib read back as the
+ * text file.
+ * gft_write_node_data / gft_read_node_data: a binary dump of a result
+ * array: the 8 bytes "GFTNODE1", u32 element type (GFT_ELEM_I32: levels,
+ * distances, labels, MIS states; GFT_ELEM_F32: PageRank ranks), u32 0, u64
+ * nnodes, then nnodes little-endian 4-byte values.  gft_read_node_data
+ * with h_val NULL only returns nnodes and the type; otherwise h_val must
+ * hold *nnodes values on entry (the capacity) and receives them. */
+#define GFT_ELEM_I32 0u
+#define GFT_ELEM_F32 1u
+GFT_API gft_status gft_write_output_gz(const char *path, uint32_t nnodes, const int32_t *h_val, int level);
+GFT_API gft_status gft_write_node_data(const char *path, uint32_t nnodes, const void *h_val, uint32_t elem_type);
+GFT_API gft_status gft_read_node_data(const char *path, uint32_t *nnodes, uint32_t *elem_type, void *h_val);
 
 #ifdef __cplusplus
 }

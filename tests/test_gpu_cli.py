@@ -106,3 +106,26 @@ def test_reference_cc_driver_with_dropin_kernel(gft, orc, tmp_path, key):
     assert comps == CC_MANIFEST[key]["components"]
     np.testing.assert_array_equal(labels, CC_VALUES[key])
     assert same_text
+
+
+@pytest.mark.parametrize("key", ["grid256.bfs.s0", "road128.sssp.s0.d10000"])
+def test_cli_gz_output_and_binary_dump(gft, tmp_path, key):
+    """`-o x.gz` writes the golden text gzip-compressed; `-b` dumps the same
+    values in binary."""
+    import gzip
+
+    e = MANIFEST[key]
+    gr = tmp_path / f"{e['graph']}.gr"
+    _graph(gft, e["recipe"], e["graph"]).write(gr)
+    z, b = tmp_path / "out.gz", tmp_path / "out.bin"
+    args = [str(CLI / e["app"]), "-o", str(z), "-b", str(b), "-s", str(e["src"])]
+    if e["app"] == "sssp":
+        args += ["-d", str(e["delta"])]
+    r = subprocess.run(args + [str(gr)], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stdout + r.stderr
+    text = gzip.decompress(z.read_bytes())
+    assert hashlib.sha256(text).hexdigest() == e["out_sha256"]
+    vals = gft.read_node_data(b)
+    want = np.array([0x7FFFFFFF if ln.split()[1] == b"INF" else int(ln.split()[1]) for ln in text.splitlines()],
+                    dtype=np.int32)
+    np.testing.assert_array_equal(vals, want)
