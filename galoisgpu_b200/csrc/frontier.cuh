@@ -39,7 +39,6 @@ struct TravParams {
     uint32_t *q[2];     // frontier / near pile
     uint32_t *far[2];   // SSSP far pile
     uint32_t *qstamp;   // SSSP: the last pile stamp per vertex (see SsspVisitorT); distances live in `out`
-    uint32_t *fused;    // SSSP bucket fusion: the distance a fused vertex was expanded at (kSolo), or NULL
     uint2 *hubs;
     uint32_t hub_cap;
     uint32_t hub_degree;
@@ -114,7 +113,6 @@ struct BfsVisitorT {
     unsigned long long claimed;
     bool vec;
 
-    __device__ __forceinline__ uint32_t vertex(uint32_t x) const { return x; }
     __device__ __forceinline__ BfsOwn owner(bool has, uint32_t u) const { return BfsOwn{u}; }
     __device__ __forceinline__ bool active(const BfsOwn &) const { return true; }
     __device__ __forceinline__ BfsOwn shfl(const BfsOwn &o, int lane) const
@@ -184,30 +182,25 @@ struct SsspOwn {
     uint32_t du;
 };
 
-// A near-pile entry with this bit set names a vertex that bucket fusion
-// already expanded in the iteration that queued it, at the distance it
-// recorded in p.fused (fusion is off on graphs of 2^31 vertices or more).
-constexpr uint32_t kFusedMark = 0x80000000u;
-
 // SSSP relaxation (apps/sssp/kernel.cu:244-259): nd = dist[u] + w; if nd
 // beats dist[v], atomicMin.  Distances are the 4-byte int32 output array
 // itself (a probe fetches a sector of eight of them, and the whole array
 // stays L2-resident on graphs of up to ~2^24 vertices).  An improvement then
-// stamps v in one 4-byte array with atomicMax, stamps increasing with the
-// iteration I: near (bucket threshold met) ((I + 1) << 1) | 1, far (I + 1)
-// << 1.
+// raises v's stamp in one 4-byte array with atomicMax.  Stamps increase with
+// the iteration I: far 4(I+1), fused 4(I+1)+1, near (bucket threshold met)
+// 4(I+1)+2.
 //   - near: v joins the near pile unless the stamp it replaced is this
 //     iteration's near stamp (so the pile holds v at most once per
 //     iteration);
 //   - far: v joins the far pile unless the stamp it replaced is from the
-//     current phase (at or after phase_stamp), which the far split also
-//     writes for the vertices it carries over.
-// With atomicMax a far stamp can never replace a near stamp of the same
-// iteration: a far improvement that loses the race to a near one is then
-// correctly dropped (v's distance is already below the threshold), and a
-// later near improvement still finds the near stamp.  Once v is near in a
-// phase it cannot go far again in that phase (distances only fall), so a
-// near stamp hides no far-pile entry.
+//     current phase (at least phase_stamp, the far stamp of the iteration
+//     that started it, which the far split writes for the vertices it
+//     carries over).
+// With atomicMax a far stamp never replaces a near (or fused) stamp of the
+// same iteration: a far improvement that loses the race to a near one is
+// dropped, rightly (v's distance is already below the threshold).  Once v is
+// near in a phase it cannot go far again in that phase (distances only
+// fall), so a near stamp hides no far-pile entry.
 //
 // kSolo: the single-query kernel's visitor, which also reads interleaved
 // (dst, weight) pairs when the graph has them, loads a vertex's row
@@ -223,32 +216,17 @@ struct SsspVisitorT {
     const uint2 *__restrict__ edge_dw;  // interleaved (dst, weight), or NULL
     uint32_t *dist;
     uint32_t *qstamp;
-    uint32_t *fused;                    // kFuse: distances at which fused vertices were expanded
-    uint32_t near_stamp, far_stamp, phase_stamp;
-    bool fusing;                        // kFuse: owner() records the distance it hands out
-    unsigned long long threshold;
-    WarpQueueT<kQB, kFuse> nq;          // near pushes (with the fused entries' upper region)
-    WarpQueueT<kQB> fq;                 // far pushes; kQB-entry buffers per warp
+    uint32_t near_stamp, phase_stamp;  // this iteration's far stamp is near_stamp - 2
+    uint32_t threshold;  // inclusive; a bucket bound above 2^32 - 1 is clamped (every distance is below it)
+    WarpQueueT<kQB> nq, fq;  // near and far pushes, kQB-entry buffers per warp
     unsigned far_min;
     unsigned long long edges;
     unsigned *err, *err_where;
     bool vec;
 
-    // The vertex of pile entry x (fused entries carry kFusedMark).
-    __device__ __forceinline__ uint32_t vertex(uint32_t x) const { return kFuse ? (x & ~kFusedMark) : x; }
-
-    // Owner of pile entry x: its distance, or INF (inactive) for a fused
-    // entry whose distance has not fallen since fusion expanded it.
-    __device__ __forceinline__ SsspOwn owner(bool has, uint32_t x) const
+    __device__ __forceinline__ SsspOwn owner(bool has, uint32_t u) const
     {
-        const uint32_t u = vertex(x);
-        if (!has) return SsspOwn{u, kInf};
-        const uint32_t du = __ldcg(dist + u);
-        if (kFuse) {
-            if ((x & kFusedMark) && __ldcg(fused + u) == du) return SsspOwn{u, kInf};
-            if (fusing) fused[u] = du;
-        }
-        return SsspOwn{u, du};
+        return SsspOwn{u, has ? __ldcg(dist + u) : kInf};
     }
     __device__ __forceinline__ bool active(const SsspOwn &o) const { return o.du != kInf; }
     __device__ __forceinline__ SsspOwn shfl(const SsspOwn &o, int lane) const
@@ -290,7 +268,7 @@ struct SsspVisitorT {
             old[k] = 0;
             if (imp[k]) {
                 if (!near[k]) far_min = min(far_min, nd[k]);
-                old[k] = atomicMax(qstamp + v[k], near[k] ? near_stamp : far_stamp);
+                old[k] = atomicMax(qstamp + v[k], near[k] ? near_stamp : near_stamp - 2u);
             }
         }
 #pragma unroll
@@ -431,9 +409,7 @@ __device__ __forceinline__ void expand_lanes(Vis &vis, const TravParams &p, bool
     // A visitor whose owner() loads per-vertex state (the SSSP distance, the
     // PageRank residual) has the row loaded alongside it, not after it: both
     // depend only on u, so the loads share one memory round trip.
-    // u is a queue entry; vis.vertex(u) is its vertex (SSSP entries may
-    // carry a mark that owner() reads).
-    const uint32_t v = vis.vertex(u);
+    const uint32_t v = u;
     uint32_t start = 0, deg = 0;
     if (Vis::kEarlyRow && has) {
         start = __ldg(p.row_start + v);
@@ -773,11 +749,14 @@ __device__ __forceinline__ void bfs_body(const TravParams &p, Mode &m, uint32_t 
 // ---------------------------------------------------------------------------
 // Bucket fusion (as in GraphIt's delta-stepping, Zhang et al., CGO 2020): a
 // warp that pushed v to the near pile in this iteration may expand v itself
-// before the barrier.  v stays in the pile, marked kFusedMark, and owner()
-// records in p.fused the distance the expansion used.  In the next
-// iteration the marked entry is skipped if v's distance is still that one,
-// and expanded again if an improvement came after.  Every read of p.fused
-// follows the write behind a barrier, so no claim protocol is needed.
+// before the barrier, taking v back out of its push buffer.  It first
+// claims v by lowering v's stamp from this iteration's near stamp to the
+// fused stamp (a compare-and-swap with acquire semantics), then reads v's
+// distance as the expansion's owner.  A later improvement of v raises the
+// stamp back to near and, having found the fused stamp, queues v again; an
+// improvement whose stamp went in before the claim is visible to the read
+// after it (the improving thread's atomicMin had completed before it issued
+// its stamp, and the claim is an acquire), so no improvement is lost.
 // Piles larger than this are not fused: every warp is busy with them
 // already, and chasing only lengthens the wait at the barrier (road
 // 4096^2 with 128-entry push buffers: 3.88 ms fusing every pile, 3.66 ms
@@ -794,8 +773,19 @@ struct SsspState {
 };
 
 // Pile stamps (see SsspVisitorT): increasing with the iteration, never 0.
-__device__ __forceinline__ uint32_t near_stamp_of(unsigned I) { return ((I + 1u) << 1) | 1u; }
-__device__ __forceinline__ uint32_t far_stamp_of(unsigned I) { return (I + 1u) << 1; }
+__device__ __forceinline__ uint32_t far_stamp_of(unsigned I) { return (I + 1u) << 2; }
+__device__ __forceinline__ uint32_t fused_stamp_of(unsigned I) { return ((I + 1u) << 2) | 1u; }
+__device__ __forceinline__ uint32_t near_stamp_of(unsigned I) { return ((I + 1u) << 2) | 2u; }
+
+__device__ __forceinline__ uint32_t cas_acquire_u32(uint32_t *p, uint32_t cmp, uint32_t val)
+{
+    uint32_t old;
+    asm volatile("atom.acquire.gpu.global.cas.b32 %0, [%1], %2, %3;"
+                 : "=r"(old)
+                 : "l"(p), "r"(cmp), "r"(val)
+                 : "memory");
+    return old;
+}
 
 // Is the coming iteration small enough for one CTA?  A near pile of at most
 // p.cta_small vertices, or a far split (empty near pile) of a far pile that
@@ -833,9 +823,8 @@ __device__ __forceinline__ int sssp_iter(const TravParams &p, Mode &m, Vis &vis,
     vis.nq.len = u32_of(ctl->qlen[nslot]);
     if (n_near > 0) {
         // Relax the near pile (apps/sssp/kernel.cu:177-306).
-        vis.threshold = T;
+        vis.threshold = (uint32_t)min(T, 0xFFFFFFFFull);
         vis.near_stamp = near_stamp_of(I);
-        vis.far_stamp = far_stamp_of(I);
         vis.phase_stamp = far_stamp_of(st.Ps);
         vis.far_min = kInf;
         vis.fq.queue = sel2(p.far, P);
@@ -846,9 +835,8 @@ __device__ __forceinline__ int sssp_iter(const TravParams &p, Mode &m, Vis &vis,
         if constexpr (Vis::kFuse) {
             // Bucket fusion: expand up to p.fuse of this warp's fresh near
             // vertices now, newest first, instead of in the next iteration.
-            // They move to the buffer's upper region, marked, and still go
-            // to the pile.
             unsigned budget = n_near <= kFuseMaxPile ? p.fuse : 0u;
+            const uint32_t fused = fused_stamp_of(I);
             while (vis.nq.count && budget) {
                 const unsigned take = min(32u, vis.nq.count);
                 const unsigned base = vis.nq.count - take;
@@ -857,10 +845,13 @@ __device__ __forceinline__ int sssp_iter(const TravParams &p, Mode &m, Vis &vis,
                 __syncwarp();
                 vis.nq.count = base;
                 budget = budget > take ? budget - take : 0;
-                vis.nq.push_top(lane < take, v | kFusedMark, lane);
-                vis.fusing = true;
+                // The claim: only this warp holds v in this iteration, so
+                // the stamp is this iteration's near stamp.  Expanding v is
+                // correct whatever the swap finds (a relaxation only ever
+                // lowers distances); the swap is what re-queues v after a
+                // later improvement.
+                if (lane < take) cas_acquire_u32(p.qstamp + v, vis.near_stamp, fused);
                 expand_lanes<Vis, SsspOwn>(vis, p, lane < take, v, &ctl->hub[slot].v, lane);
-                vis.fusing = false;
             }
         }
         vis.nq.flush(lane);
@@ -969,24 +960,17 @@ __device__ __forceinline__ void sssp_body(const TravParams &p, Mode &m, uint32_t
     vis.edge_dw = p.edge_dw;
     vis.dist = dist;
     vis.qstamp = p.qstamp;
-    vis.fused = p.fused;
-    vis.fusing = false;
     vis.edges = 0;
     vis.err = &ctl->error;
     vis.err_where = &ctl->error_where;
     vis.vec = p.vec_ok;
     vis.nq.buf = near_buf;
     vis.nq.count = 0;
-    vis.nq.top = kQB;
     vis.nq.cap = p.qcap;
     vis.nq.err = &ctl->error;
     vis.nq.err_where = &ctl->error_where;
+    vis.fq = vis.nq;
     vis.fq.buf = far_buf;
-    vis.fq.count = 0;
-    vis.fq.top = kQB;
-    vis.fq.cap = p.qcap;
-    vis.fq.err = &ctl->error;
-    vis.fq.err_where = &ctl->error_where;
 
     SsspState st{p.delta, 0, 0, 0};
     for (;;) {

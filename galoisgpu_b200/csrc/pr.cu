@@ -63,7 +63,6 @@ struct PrInitVisitor {
     unsigned long long edges;
     bool vec;
 
-    __device__ __forceinline__ uint32_t vertex(uint32_t x) const { return x; }
     __device__ __forceinline__ PrOwn owner(bool has, uint32_t u) const
     {
         if (!has) return PrOwn{u, 0.f};
@@ -127,7 +126,6 @@ struct PrVisitor {
     unsigned long long edges;
     bool vec;
 
-    __device__ __forceinline__ uint32_t vertex(uint32_t x) const { return x; }
     __device__ __forceinline__ PrOwn owner(bool has, uint32_t u)
     {
         if (!has) return PrOwn{u, 0.f};

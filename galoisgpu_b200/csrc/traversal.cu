@@ -472,14 +472,13 @@ gft_status run_traversal(bool is_sssp, gft_engine *e, const gft_graph *g, uint32
     };
     size_t o_q0 = take((size_t)qcap * 4), o_q1 = take((size_t)qcap * 4);
     size_t o_hubs = take((size_t)hub_cap * 8);
-    size_t o_vis = 0, o_f0 = 0, o_f1 = 0, o_qs = 0, o_fu = 0;
+    size_t o_vis = 0, o_f0 = 0, o_f1 = 0, o_qs = 0;
     if (is_sssp) {
         // Distances are computed in place in d_out; per vertex the engine
-        // keeps a pile stamp and, for bucket fusion, a fused distance.
+        // keeps only a pile stamp.
         o_f0 = take((size_t)qcap * 4);
         o_f1 = take((size_t)qcap * 4);
         o_qs = take((size_t)n * 4);
-        o_fu = take((size_t)n * 4);
     } else {
         o_vis = take((size_t)((n + 31) / 32) * 4);
     }
@@ -502,7 +501,6 @@ gft_status run_traversal(bool is_sssp, gft_engine *e, const gft_graph *g, uint32
         p.far[0] = reinterpret_cast<uint32_t *>(base + o_f0);
         p.far[1] = reinterpret_cast<uint32_t *>(base + o_f1);
         p.qstamp = reinterpret_cast<uint32_t *>(base + o_qs);
-        p.fused = reinterpret_cast<uint32_t *>(base + o_fu);
     } else {
         p.visited = reinterpret_cast<uint32_t *>(base + o_vis);
     }
@@ -520,7 +518,6 @@ gft_status run_traversal(bool is_sssp, gft_engine *e, const gft_graph *g, uint32
     if (is_sssp && !single)
         p.cta_small = t.cta_small == UINT32_MAX ? 0 : t.cta_small ? t.cta_small : p.uniform ? kDefaultCtaSmall : 0;
     if (is_sssp) p.fuse = t.fuse == UINT32_MAX ? 0 : t.fuse ? t.fuse : p.uniform ? kDefaultFuse : 0;
-    if (n > dev::kFusedMark) p.fuse = 0;  // fused pile entries carry their mark in the top id bit
 
     GFT_CUDA_TRY(cudaMemsetAsync(e->ctl.ptr, 0, sizeof(TraversalCtl), stream));
     void *args[] = {&p};

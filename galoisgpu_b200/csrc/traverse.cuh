@@ -158,10 +158,7 @@ static_assert(kQueueBuf >= 64 && kQueueBuf % 32 == 0, "queue buffer: a multiple 
 // Warp-aggregated append to a global queue through a CAP-entry per-warp
 // shared-memory buffer: one atomic reservation per flush.  `count` is warp
 // uniform.  All 32 lanes must call push() and flush() together.
-// kTop: a second region, [top, CAP), filled downwards by push_top(), goes
-// out with the same flush; entries there are not part of [0, count), which
-// a caller may take back (SSSP bucket fusion takes its vertices from there).
-template <unsigned CAP, bool kTop = false>
+template <unsigned CAP>
 struct WarpQueueT {
     static_assert(CAP >= 64 && CAP % 32 == 0, "queue buffer: a multiple of 32, at least 64");
     uint32_t *buf;       // this warp's CAP shared-memory slots
@@ -170,28 +167,21 @@ struct WarpQueueT {
     unsigned *len;       // global length counter
     unsigned cap;        // capacity of `queue`
     unsigned *err, *err_where;
-    unsigned top;        // kTop: first entry of the upper region (CAP = empty); unused otherwise
-
-    __device__ __forceinline__ unsigned held() const { return kTop ? count + (CAP - top) : count; }
 
     __device__ __forceinline__ void flush(unsigned lane)
     {
-        const unsigned n = held();
-        if (n == 0) return;
+        if (count == 0) return;
         __syncwarp();
         unsigned base = 0;
-        if (lane == 0) base = atomicAdd(len, n);
+        if (lane == 0) base = atomicAdd(len, count);
         base = __shfl_sync(kFull, base, 0);
-        if (base + n > cap) {
+        if (base + count > cap) {
             if (lane == 0) raise_error(err, err_where, GFT_ERR_OVERFLOW, base);
         } else {
             for (unsigned i = lane; i < count; i += 32) queue[base + i] = buf[i];
-            if (kTop)
-                for (unsigned i = lane; i < CAP - top; i += 32) queue[base + count + i] = buf[top + i];
         }
         __syncwarp();
         count = 0;
-        top = CAP;
     }
 
     __device__ __forceinline__ void push(bool p, uint32_t item, unsigned lane)
@@ -200,17 +190,7 @@ struct WarpQueueT {
         if (mask == 0) return;
         if (p) buf[count + __popc(mask & lanemask_lt())] = item;
         count += __popc(mask);
-        if (held() > CAP - 32) flush(lane);
-    }
-
-    __device__ __forceinline__ void push_top(bool p, uint32_t item, unsigned lane)
-    {
-        static_assert(kTop, "push_top needs the upper region");
-        unsigned mask = __ballot_sync(kFull, p);
-        if (mask == 0) return;
-        if (p) buf[top - 1 - __popc(mask & lanemask_lt())] = item;
-        top -= __popc(mask);
-        if (held() > CAP - 32) flush(lane);
+        if (count > CAP - 32) flush(lane);
     }
 };
 using WarpQueue = WarpQueueT<kQueueBuf>;
