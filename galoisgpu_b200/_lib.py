@@ -144,6 +144,8 @@ class ServeConfig(C.Structure):
         ("max_lanes_per_request", C.c_uint32),
         ("wide_lanes", C.c_uint32),
         ("wide_min_edges", C.c_uint32),
+        ("resident", C.c_uint32),
+        ("idle_exit_us", C.c_uint32),
     ]
 
 

@@ -42,11 +42,12 @@ LIB_SOURCES = [
     "batch.cu",
     "msbfs.cu",
     "serve.cpp",
+    "resident.cu",
     "cc.cu",
     "pr.cu",
     "mis.cu",
 ]
-HEADERS = ["gft_internal.h", "gen_common.h", "traverse.cuh", "frontier.cuh"]
+HEADERS = ["gft_internal.h", "gen_common.h", "traverse.cuh", "frontier.cuh", "job.cuh"]
 CLI_SOURCE = "cli_main.cpp"
 
 NVCC_FLAGS = [

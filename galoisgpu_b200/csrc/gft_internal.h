@@ -177,6 +177,16 @@ struct DeviceScope {
 // is being captured, the graph keeps the separate arrays only.
 gft_status ensure_edge_pairs(gft_graph *g, cudaStream_t stream);
 gft_status graph_degree_stats(DeviceGraph &G, cudaStream_t stream);
+// Resident-kernel serving (resident.cu), behind gft_serve_* when
+// gft_serve_config.resident is set.
+struct ResidentServer;
+gft_status resident_open(gft_engine *e, const gft_serve_config &cfg, ResidentServer **out);
+const gft_serve_config &resident_config(const ResidentServer *s);
+gft_status resident_enqueue(ResidentServer *s, const gft_query &q, size_t scratch_bytes, uint64_t *ticket);
+gft_status resident_poll(ResidentServer *s, gft_completion *out, uint32_t max, uint32_t *n, uint32_t wait_us);
+void resident_stats(ResidentServer *s, uint64_t *in_flight, uint64_t *launches, uint64_t *queries);
+void resident_close(ResidentServer *s);
+
 // Index of the first edge whose destination is >= nnodes (~0 if none).
 gft_status check_edges_device(const DeviceGraph &G, cudaStream_t stream, uint64_t *first_bad);
 // Graphs whose out-degrees are all at most this many edges have near-equal

@@ -79,6 +79,7 @@ struct gft_server {
     std::atomic<bool> stop{false};
     std::thread dispatcher;
     uint64_t launched_batches = 0, launched_queries = 0;
+    gft::ResidentServer *rs = nullptr;  // resident mode: everything below is its job
 };
 
 using namespace gft;
@@ -304,6 +305,16 @@ gft_status gft_serve_open(gft_engine *e, const gft_serve_config *cfg_in, gft_ser
     if (cfg.max_batch == 0 || cfg.lane_arena_bytes == 0 || cfg.queue_capacity == 0)
         return fail(GFT_ERR_INVALID_ARG, "gft_serve_open: arena, batch and queue sizes must be > 0");
     if (cfg.hub_degree < 32) cfg.hub_degree = 32;
+    if (cfg.resident) {
+        gft::ResidentServer *rs = nullptr;
+        GFT_TRY(gft::resident_open(e, cfg, &rs));
+        gft_server *s = new gft_server();
+        s->engine = e;
+        s->rs = rs;
+        s->cfg = gft::resident_config(rs);
+        *out = s;
+        return GFT_OK;
+    }
     gft_server *s = new gft_server();
     s->engine = e;
     s->cfg = cfg;
@@ -352,6 +363,7 @@ gft_status gft_serve_enqueue(gft_server *s, const gft_query *q, uint64_t *ticket
     if (!q->graph || !q->d_out || q->app > 1 || (q->app == 1 && q->delta <= 0) || q->src >= q->graph->g.nnodes ||
         q->graph->g.device != s->engine->device)
         return fail(GFT_ERR_INVALID_ARG, "gft_serve_enqueue: invalid query");
+    if (s->rs) return resident_enqueue(s->rs, *q, req_scratch(*q, s->cfg.hub_degree), ticket);
     if (req_scratch(*q, s->cfg.hub_degree) > s->cfg.lane_arena_bytes)
         return fail(GFT_ERR_OOM, "gft_serve_enqueue: the query's scratch exceeds a lane arena (%zu bytes)",
                     s->cfg.lane_arena_bytes);
@@ -373,6 +385,7 @@ gft_status gft_serve_enqueue(gft_server *s, const gft_query *q, uint64_t *ticket
 gft_status gft_serve_poll(gft_server *s, gft_completion *out, uint32_t max, uint32_t *n, uint32_t wait_us)
 {
     if (!s || !n || (max && !out)) return fail(GFT_ERR_INVALID_ARG, "gft_serve_poll: null argument");
+    if (s->rs) return resident_poll(s->rs, out, max, n, wait_us);
     std::unique_lock<std::mutex> lk(s->mu);
     if (s->done.empty() && wait_us)
         s->cv_done.wait_for(lk, std::chrono::microseconds(wait_us), [&] { return !s->done.empty(); });
@@ -388,6 +401,10 @@ gft_status gft_serve_poll(gft_server *s, gft_completion *out, uint32_t max, uint
 gft_status gft_serve_stats(gft_server *s, uint64_t *in_flight, uint64_t *batches, uint64_t *queries)
 {
     if (!s) return fail(GFT_ERR_INVALID_ARG, "gft_serve_stats: server is NULL");
+    if (s->rs) {
+        resident_stats(s->rs, in_flight, batches, queries);
+        return GFT_OK;
+    }
     std::lock_guard<std::mutex> lk(s->mu);
     if (in_flight) *in_flight = s->in_flight;
     if (batches) *batches = s->launched_batches;
@@ -398,6 +415,11 @@ gft_status gft_serve_stats(gft_server *s, uint64_t *in_flight, uint64_t *batches
 gft_status gft_serve_close(gft_server *s)
 {
     if (!s) return GFT_OK;
+    if (s->rs) {
+        resident_close(s->rs);
+        delete s;
+        return GFT_OK;
+    }
     {
         std::lock_guard<std::mutex> lk(s->mu);
         s->stop = true;

@@ -394,6 +394,16 @@ typedef struct gft_serve_config {
                                    4/9 of the lanes when there are >= 4; 0 =
                                    no pool)                                   */
     uint32_t wide_min_edges;    /* default 2^25                                */
+    uint32_t resident;          /* 1: one resident persistent kernel takes the
+                                   requests from a ring in mapped host memory
+                                   and runs each on a team of lanes drafted on
+                                   the device (lane_blocks CTAs per lane,
+                                   default 8; widths as idle lanes / waiting
+                                   requests, at most max_lanes_per_request);
+                                   0: one launch per lane micro-batch (default) */
+    uint32_t idle_exit_us;      /* resident: the kernel ends after this long
+                                   without work and is launched again by the
+                                   next request (0 = 2000)                    */
 } gft_serve_config;
 #define GFT_SERVE_AUTO 0xFFFFFFFFu
 

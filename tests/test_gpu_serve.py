@@ -133,3 +133,95 @@ def test_wide_pool_for_skewed_sssp(gft, engine):
         assert got[t]["status"] == 0
         alone = (engine.sssp(devs[gi], src, delta=300) if app == "sssp" else engine.bfs(devs[gi], src))["out"]
         np.testing.assert_array_equal(out.cpu().numpy(), alone.cpu().numpy())
+
+
+# ---------------------------------------------------------------------------
+# Resident mode: one persistent kernel, requests through a mapped ring, teams
+# of lanes drafted on the device.
+# ---------------------------------------------------------------------------
+def test_resident_mix_equals_alone(gft, engine):
+    import torch
+
+    from galoisgpu_b200.serve import Server
+
+    hosts = [gft.CSRGraph.road(60, seed=21), gft.CSRGraph.road(200, seed=22),
+             gft.CSRGraph.rmat(11, 8, seed=23, max_weight=255), gft.CSRGraph.rmat(14, 8, seed=24, max_weight=255),
+             gft.CSRGraph.grid(30, 30, 0, 7)]
+    devs = [h.copy_to_gpu() for h in hosts]
+    srv = Server(engine, resident=1, lane_blocks=8, lane_arena_bytes=64 << 20)
+    reqs = []
+    for i in range(160):
+        gi = i % len(devs)
+        src = hosts[gi].pick_sources(300 + i, 1)[0]
+        app = "sssp" if i % 3 else "bfs"
+        out = torch.full((devs[gi].nnodes,), -5, dtype=torch.int32, device="cuda")
+        d = [100, 40000][i % 2]
+        reqs.append((srv.enqueue(devs[gi], app, src, out, delta=d), gi, app, src, out, d))
+    got = drain(srv, len(reqs))
+    st = srv.stats()
+    srv.close()
+    assert all(c["status"] == 0 for c in got.values()), [c["status"] for c in got.values() if c["status"]]
+    assert len({c["lane"] for c in got.values()}) > 1, "requests never ran on several teams at once"
+    assert st["batches"] < st["queries"], "one kernel launch per request: the kernel did not stay resident"
+    for t, gi, app, src, out, delta in reqs:
+        alone = (engine.sssp(devs[gi], src, delta=delta) if app == "sssp" else engine.bfs(devs[gi], src))["out"]
+        np.testing.assert_array_equal(out.cpu().numpy(), alone.cpu().numpy())
+
+
+def test_resident_idle_server_gives_a_request_every_lane_and_relaunches(gft, engine):
+    import torch
+
+    from galoisgpu_b200.serve import Server
+
+    h = gft.CSRGraph.road(300, seed=5)
+    d = h.copy_to_gpu()
+    srv = Server(engine, resident=1, lane_blocks=8, lane_arena_bytes=64 << 20, idle_exit_us=1000)
+    lanes = srv.config["lanes"]
+    outs = []
+    for k in range(2):
+        out = torch.empty(d.nnodes, dtype=torch.int32, device="cuda")
+        srv.enqueue(d, "sssp", 3 + k, out, delta=1000)
+        c = list(drain(srv, 1).values())[0]
+        assert c["status"] == 0 and c["width"] == lanes, c
+        outs.append(out)
+        time.sleep(0.05)  # longer than idle_exit_us: the kernel ends and the next request launches it again
+    st = srv.stats()
+    srv.close()
+    assert st["batches"] == 2, st
+    for k, out in enumerate(outs):
+        np.testing.assert_array_equal(out.cpu().numpy(), engine.sssp(d, 3 + k, delta=1000)["out"].cpu().numpy())
+
+
+def test_resident_close_finishes_admitted_requests(gft, engine):
+    import torch
+
+    from galoisgpu_b200.serve import Server
+
+    h = gft.CSRGraph.rmat(13, 8, seed=41, max_weight=255)
+    d = h.copy_to_gpu()
+    srv = Server(engine, resident=1, lane_arena_bytes=64 << 20)
+    srcs = h.pick_sources(9, 24)
+    outs = [torch.full((d.nnodes,), -5, dtype=torch.int32, device="cuda") for _ in srcs]
+    for s, o in zip(srcs, outs):
+        srv.enqueue(d, "bfs", s, o)
+    srv.close()
+    for s, o in zip(srcs, outs):
+        np.testing.assert_array_equal(o.cpu().numpy(), engine.bfs(d, s)["out"].cpu().numpy())
+
+
+def test_resident_admission_errors(gft, engine):
+    import torch
+
+    from galoisgpu_b200.serve import Server
+
+    h = gft.CSRGraph.road(300, seed=3)
+    d = h.copy_to_gpu()
+    srv = Server(engine, resident=1, lane_arena_bytes=1 << 16)
+    out = torch.empty(d.nnodes, dtype=torch.int32, device="cuda")
+    with pytest.raises(gft.GftError) as ei:
+        srv.enqueue(d, "sssp", 0, out)
+    assert ei.value.status_name == "GFT_ERR_OOM"
+    with pytest.raises(gft.GftError) as ei:
+        srv.enqueue(d, "bfs", d.nnodes, out)
+    assert ei.value.status_name == "GFT_ERR_INVALID_ARG"
+    srv.close()
