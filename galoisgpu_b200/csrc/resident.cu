@@ -33,6 +33,13 @@
 // control block (the block is reused only once every member has left it),
 // and each lane's first CTA puts its lane back into the idle set.
 //
+// Ordering.  A request goes through no CUDA stream, so nothing orders it
+// with other work: whatever writes its buffers (say, a fill kernel on another
+// stream) must have finished before it is enqueued, and its results are
+// ready once its completion is polled.  Kernels launched on other streams
+// while the resident kernel holds the SMs wait until it ends (it leaves
+// after idle_exit_us without work).
+//
 // Waits.  Every device wait is bounded: team barriers by the engine's
 // barrier timeout, mailbox and ring polls by the idle limit, after which an
 // idle lane leaves the kernel (it takes its own bit out of the idle set
@@ -120,6 +127,57 @@ __device__ __forceinline__ void st_release_sys_u32(unsigned *p, unsigned v)
     asm volatile("st.release.sys.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
+// Bumps a mailbox sequence number with release semantics.  An atomic, so
+// that the writer never works from a stale copy of the number (a plain load
+// could hit this SM's L1 while another SM's leader has bumped it since).
+__device__ __forceinline__ void bump_release_u32(unsigned *p)
+{
+    unsigned old;
+    asm volatile("atom.release.gpu.global.add.u32 %0, [%1], 1;" : "=r"(old) : "l"(p) : "memory");
+}
+
+// Copies a job out of the mapped ring with system-scope loads, so that no
+// line this SM cached earlier (a neighbouring slot shares it) is used.
+__device__ __forceinline__ void load_ring_job(BatchJob *dst, const BatchJob *src)
+{
+    static_assert(sizeof(BatchJob) % 8 == 0, "BatchJob is copied in 8-byte words");
+    const unsigned long long *s = reinterpret_cast<const unsigned long long *>(src);
+    unsigned long long *d = reinterpret_cast<unsigned long long *>(dst);
+#pragma unroll
+    for (unsigned i = 0; i < sizeof(BatchJob) / 8; i++) {
+        unsigned long long v;
+        asm volatile("ld.relaxed.sys.global.u64 %0, [%1];" : "=l"(v) : "l"(s + i) : "memory");
+        d[i] = v;
+    }
+}
+
+// Copies a job from device memory with L2 (coherent) loads: the team's CTAs
+// run on SMs whose L1 may still hold an earlier job of the same control
+// block.
+__device__ __forceinline__ void load_job_cg(BatchJob *dst, const BatchJob *src)
+{
+    const unsigned long long *s = reinterpret_cast<const unsigned long long *>(src);
+    unsigned long long *d = reinterpret_cast<unsigned long long *>(dst);
+#pragma unroll
+    for (unsigned i = 0; i < sizeof(BatchJob) / 8; i++) d[i] = __ldcg(s + i);
+}
+
+#ifdef GFT_RESIDENT_TRACE
+// Diagnostic builds only: (time, lane << 48 | event << 40 | value) records.
+__device__ unsigned long long g_rtrace[2 * 65536];
+__device__ unsigned g_rtrace_n;
+__device__ __forceinline__ void rtrace(unsigned lane, unsigned ev, unsigned long long v)
+{
+    const unsigned i = atomicAdd(&g_rtrace_n, 1u);
+    if (i < 65536) {
+        g_rtrace[2 * i] = globaltimer_ns();
+        g_rtrace[2 * i + 1] = ((unsigned long long)lane << 48) | ((unsigned long long)ev << 40) | (v & 0xFFFFFFFFFFull);
+    }
+}
+#else
+__device__ __forceinline__ void rtrace(unsigned, unsigned, unsigned long long) {}
+#endif
+
 struct ResArgs {
     ResDev *S;
     ResHost *H;
@@ -190,7 +248,7 @@ __device__ bool lead_team(const ResArgs &a, unsigned lane, unsigned long long h,
     ResTeam &T = S->team[lane];
     // The control block is free once every CTA of its last job left it.
     const unsigned long long t0 = globaltimer_ns();
-    while (ld_acquire_u32(&T.left) != T.members) {
+    while (ld_acquire_u32(&T.left) != __ldcg(&T.members)) {
         if (globaltimer_ns() - t0 > a.timeout_ns) {
             if (got) atomicOr(&S->idle, got);
             // The job cannot run here: report it.
@@ -209,7 +267,7 @@ __device__ bool lead_team(const ResArgs &a, unsigned lane, unsigned long long h,
     T.members = team_lanes * a.lane_ctas;
     T.index = (unsigned)h;
     T.t_claim = globaltimer_ns();
-    T.job = a.ring[h % a.ring_size];  // from mapped host memory
+    load_ring_job(&T.job, a.ring + h % a.ring_size);  // from mapped host memory
     __threadfence();
     // Commands: this lane is rank 0, the drafted lanes follow in lane order.
     unsigned rank = 0;
@@ -221,8 +279,9 @@ __device__ bool lead_team(const ResArgs &a, unsigned lane, unsigned long long h,
         b.team_lane = lane;
         b.team_lanes = team_lanes;
         b.rank = l == lane ? 0u : ++rank;
-        st_release_u32(&b.seq, b.seq + 1);
+        bump_release_u32(&b.seq);
     }
+    rtrace(lane, 1, (h << 8) | team_lanes);
     return true;
 }
 
@@ -236,13 +295,26 @@ __device__ void lane_leader_idle(const ResArgs &a, unsigned lane, unsigned seen,
     ResDev *S = a.S;
     const unsigned long long mine = 1ull << lane;
     unsigned sleep_ns = 32;
+    unsigned long long t_drafted = 0;  // when the lane was first found drafted without its command yet
     for (;;) {
         if (ld_acquire_u32(&S->box[lane].seq) != seen) return;
+        if (t_drafted && globaltimer_ns() - t_drafted > a.timeout_ns) {
+            // A drafter took this lane but its command never came: leave, so
+            // that the wait is bounded (the team's own barrier times out).
+            ResLaneBox &b = S->box[lane];
+            b.cmd = kCmdExit;
+            bump_release_u32(&b.seq);
+            rtrace(lane, 6, 0);
+            return;
+        }
         const unsigned long long tail = ld_acquire_sys_u64(&a.H->tail);
         const unsigned head = ld_relaxed_u32(&S->head);
         if (head < tail) {
             const unsigned long long old = atomicAnd(&S->idle, ~mine);
-            if (!(old & mine)) continue;  // drafted meanwhile: the mailbox has the command
+            if (!(old & mine)) {  // drafted meanwhile: the mailbox gets the command
+                if (!t_drafted) t_drafted = globaltimer_ns();
+                continue;
+            }
             if (atomicCAS(&S->head, head, head + 1) == head) {
                 if (!lead_team(a, lane, head, tail)) atomicOr(&S->idle, mine);
             } else {
@@ -257,9 +329,11 @@ __device__ void lane_leader_idle(const ResArgs &a, unsigned lane, unsigned seen,
             if (old & mine) {  // out of the idle set: nobody can draft this lane now
                 ResLaneBox &b = S->box[lane];
                 b.cmd = kCmdExit;
-                st_release_u32(&b.seq, b.seq + 1);
+                bump_release_u32(&b.seq);
+                rtrace(lane, 5, 0);
                 return;
             }
+            if (!t_drafted) t_drafted = globaltimer_ns();
             continue;  // drafted
         }
         __nanosleep(sleep_ns);
@@ -274,6 +348,7 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) serve_resident(ResArgs a)
     __shared__ uint32_t s_near[BLOCK / 32][QB];
     __shared__ uint32_t s_far[BLOCK / 32][QB];
     __shared__ TravParams s_p;
+    __shared__ BatchJob s_jb;
     __shared__ unsigned s_app, s_cmd, s_job, s_team_lane, s_team_lanes, s_rank;
     __shared__ unsigned long long s_t0;
     const unsigned lane = blockIdx.x / a.lane_ctas, r = blockIdx.x % a.lane_ctas;
@@ -299,13 +374,16 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) serve_resident(ResArgs a)
                 sleep_ns = min(sleep_ns * 2, 512u);
                 s = ld_acquire_u32(&S->box[lane].seq);
             }
-            const ResLaneBox &b = S->box[lane];
-            s_cmd = s == seen ? kCmdExit : b.cmd;
+            // The mailbox fields through L2 (see load_job_cg).
+            ResLaneBox *b = &S->box[lane];
+            s_cmd = s == seen ? kCmdExit : __ldcg(&b->cmd);
+            if (s == seen) rtrace(lane, 7, r);
             seen = s;
-            s_job = b.job;
-            s_team_lane = b.team_lane;
-            s_team_lanes = b.team_lanes;
-            s_rank = b.rank;
+            s_job = __ldcg(&b->job);
+            s_team_lane = __ldcg(&b->team_lane);
+            s_team_lanes = __ldcg(&b->team_lanes);
+            s_rank = __ldcg(&b->rank);
+            if (r == 0) rtrace(lane, 2, ((unsigned long long)s_job << 16) | (s_rank << 8) | s_cmd);
         }
         __syncthreads();
         if (s_cmd != kCmdRun) return;
@@ -313,8 +391,9 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) serve_resident(ResArgs a)
         const unsigned team_ctas = s_team_lanes * a.lane_ctas;
         const unsigned rank_cta = s_rank * a.lane_ctas + r;
         if (threadIdx.x == 0) {
-            s_p = job_params(T.job, a.arenas + (size_t)s_team_lane * a.arena_bytes, a.hub_degree, &T.ctl);
-            s_app = T.job.app;
+            load_job_cg(&s_jb, &T.job);
+            s_p = job_params(s_jb, a.arenas + (size_t)s_team_lane * a.arena_bytes, a.hub_degree, &T.ctl);
+            s_app = s_jb.app;
             s_t0 = globaltimer_ns();
         }
         __syncthreads();
@@ -329,18 +408,20 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) serve_resident(ResArgs a)
         gs.sync();  // the whole team is done with the traversal
         if (threadIdx.x == 0) {
             if (rank_cta == 0) {
-                ResDone &d = a.done[T.index % a.ring_size];
+                const unsigned index = __ldcg(&T.index);
+                ResDone &d = a.done[index % a.ring_size];
                 d.status = ld_relaxed_u32(&ctl->error);
-                d.levels = ctl->levels;
-                d.iterations = ctl->iterations;
-                d.edges = ctl->edges;
-                d.t_claim = T.t_claim;
+                d.levels = __ldcg(&ctl->levels);
+                d.iterations = __ldcg(&ctl->iterations);
+                d.edges = __ldcg(&ctl->edges);
+                d.t_claim = __ldcg(&T.t_claim);
                 d.t_start = s_t0;
                 d.t_end = globaltimer_ns();
                 d.lane = s_team_lane;
                 d.width = s_team_lanes;
                 __threadfence_system();  // the record and the results before the sequence number
-                st_release_sys_u32(&d.seq, T.index + 1);
+                st_release_sys_u32(&d.seq, index + 1);
+                rtrace(lane, 3, ((unsigned long long)index << 8) | d.status);
             }
             atomicAdd(&T.left, 1u);  // after this the block may be reset for the next job
             if (r == 0) {
@@ -363,6 +444,18 @@ const void *resident_kernel_ptr(int block)
 }
 
 }  // namespace dev
+
+#ifdef GFT_RESIDENT_TRACE
+extern "C" GFT_API int gft_debug_resident_trace(unsigned long long *host, int max_records)
+{
+    unsigned n = 0;
+    if (cudaMemcpyFromSymbol(&n, dev::g_rtrace_n, sizeof n) != cudaSuccess) return -1;
+    n = std::min<unsigned>(n, 65536u);
+    n = std::min<unsigned>(n, (unsigned)max_records);
+    if (n && cudaMemcpyFromSymbol(host, dev::g_rtrace, sizeof(unsigned long long) * 2 * n) != cudaSuccess) return -1;
+    return (int)n;
+}
+#endif
 
 namespace {
 

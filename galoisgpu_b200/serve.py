@@ -38,7 +38,9 @@ class Server:
 
     def enqueue(self, graph: DeviceGraph, app: str, src: int, out, delta: int = DEFAULT_DELTA, parent=None) -> int:
         """Admits one request; `out` (int32 device tensor of graph.nnodes) must
-        stay alive until the request's completion is polled."""
+        stay alive until the request's completion is polled.  With
+        resident=1 the request is ordered with no stream: any pending work
+        that writes `out` must have finished first."""
         q = self._q
         q.graph = graph.handle
         q.app = 1 if app == "sssp" else 0

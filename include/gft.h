@@ -400,7 +400,13 @@ typedef struct gft_serve_config {
                                    the device (lane_blocks CTAs per lane,
                                    default 8; widths as idle lanes / waiting
                                    requests, at most max_lanes_per_request);
-                                   0: one launch per lane micro-batch (default) */
+                                   0: one launch per lane micro-batch (default).
+                                   A resident request is ordered with no
+                                   stream: work that writes its buffers must
+                                   be finished before gft_serve_enqueue, and
+                                   kernels launched meanwhile on other
+                                   streams wait until the resident kernel
+                                   ends (idle_exit_us after its last work) */
     uint32_t idle_exit_us;      /* resident: the kernel ends after this long
                                    without work and is launched again by the
                                    next request (0 = 2000)                    */

@@ -148,15 +148,17 @@ def test_resident_mix_equals_alone(gft, engine):
              gft.CSRGraph.rmat(11, 8, seed=23, max_weight=255), gft.CSRGraph.rmat(14, 8, seed=24, max_weight=255),
              gft.CSRGraph.grid(30, 30, 0, 7)]
     devs = [h.copy_to_gpu() for h in hosts]
-    srv = Server(engine, resident=1, lane_blocks=8, lane_arena_bytes=64 << 20)
-    reqs = []
+    # Resident requests are ordered with no stream: the outputs' fills must
+    # be finished before the requests are enqueued.
+    plan = []
     for i in range(160):
         gi = i % len(devs)
         src = hosts[gi].pick_sources(300 + i, 1)[0]
-        app = "sssp" if i % 3 else "bfs"
         out = torch.full((devs[gi].nnodes,), -5, dtype=torch.int32, device="cuda")
-        d = [100, 40000][i % 2]
-        reqs.append((srv.enqueue(devs[gi], app, src, out, delta=d), gi, app, src, out, d))
+        plan.append((gi, "sssp" if i % 3 else "bfs", src, out, [100, 40000][i % 2]))
+    torch.cuda.synchronize()
+    srv = Server(engine, resident=1, lane_blocks=8, lane_arena_bytes=64 << 20)
+    reqs = [(srv.enqueue(devs[gi], app, src, out, delta=d), gi, app, src, out, d) for gi, app, src, out, d in plan]
     got = drain(srv, len(reqs))
     st = srv.stats()
     srv.close()
@@ -202,6 +204,7 @@ def test_resident_close_finishes_admitted_requests(gft, engine):
     srv = Server(engine, resident=1, lane_arena_bytes=64 << 20)
     srcs = h.pick_sources(9, 24)
     outs = [torch.full((d.nnodes,), -5, dtype=torch.int32, device="cuda") for _ in srcs]
+    torch.cuda.synchronize()  # the fills finish before the requests reach the resident kernel
     for s, o in zip(srcs, outs):
         srv.enqueue(d, "bfs", s, o)
     srv.close()
