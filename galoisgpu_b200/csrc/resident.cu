@@ -40,12 +40,13 @@
 // while the resident kernel holds the SMs wait until it ends (it leaves
 // after idle_exit_us without work).
 //
-// Waits.  Every device wait is bounded: team barriers by the engine's
-// barrier timeout, mailbox and ring polls by the idle limit, after which an
-// idle lane leaves the kernel (it takes its own bit out of the idle set
-// first, so it is never drafted after leaving).  The kernel ends when all
-// lanes have left; the host launches it again when a job is published and
-// no kernel is running.
+// Waits.  Every device wait is bounded.  Team barriers time out after the
+// engine's barrier limit.  The kernel closes as a whole once every lane has
+// been idle for idle_exit_us (or the host asked it to stop and no job
+// waits): each lane then takes its own bit out of the idle set, so it is
+// never drafted after leaving, and posts its own exit command, which ends
+// the lane's waiting CTAs.  The host launches the kernel again when a job
+// is published and no kernel is running.
 #include <string.h>
 
 #include <algorithm>
@@ -85,9 +86,11 @@ struct alignas(128) ResTeam {
 
 // Device memory.
 struct ResDev {
-    unsigned long long idle;  // bit per lane that is idle and may be drafted
-    unsigned head;            // next ring index to claim (persists across launches)
-    unsigned pad[29];
+    unsigned long long idle;       // bit per lane that is idle and may be drafted
+    unsigned long long last_busy;  // %globaltimer of the last claim or completion (0 at launch)
+    unsigned head;                 // next ring index to claim (persists across launches)
+    unsigned closing;              // set once: every lane leaves as soon as it is idle
+    unsigned pad[26];
     ResLaneBox box[kResMaxLanes];
     ResTeam team[kResMaxLanes];
 };
@@ -190,6 +193,7 @@ struct ResArgs {
     char *arenas;
     unsigned long long arena_bytes;
     uint32_t hub_degree;
+    unsigned long long all_lanes;  // the idle mask with every lane in it
     unsigned long long idle_ns;
     unsigned long long timeout_ns;
 };
@@ -287,10 +291,13 @@ __device__ bool lead_team(const ResArgs &a, unsigned lane, unsigned long long h,
 
 // Thread 0 of a lane's first CTA while its lane is idle: claims jobs and
 // leads teams until the lane has a command of its own (which it returns
-// through the mailbox).  Leaves the idle set and posts kCmdExit for its
-// lane after `idle_ns` without work, or once the host asked to stop and no
-// job waits.
-__device__ void lane_leader_idle(const ResArgs &a, unsigned lane, unsigned seen, unsigned long long &t_idle)
+// through the mailbox).  The kernel closes as a whole: once every lane has
+// been idle for `idle_ns` (or the host asked to stop and no job waits), the
+// first lane to see it sets `closing`, and from then on every lane leaves
+// the idle set and posts kCmdExit for itself as soon as it is idle.  (A lane
+// leaving on its own would take its share of the device away until the
+// whole kernel ended.)
+__device__ void lane_leader_idle(const ResArgs &a, unsigned lane, unsigned seen, unsigned long long t_start)
 {
     ResDev *S = a.S;
     const unsigned long long mine = 1ull << lane;
@@ -307,24 +314,35 @@ __device__ void lane_leader_idle(const ResArgs &a, unsigned lane, unsigned seen,
             rtrace(lane, 6, 0);
             return;
         }
-        const unsigned long long tail = ld_acquire_sys_u64(&a.H->tail);
-        const unsigned head = ld_relaxed_u32(&S->head);
-        if (head < tail) {
-            const unsigned long long old = atomicAnd(&S->idle, ~mine);
-            if (!(old & mine)) {  // drafted meanwhile: the mailbox gets the command
-                if (!t_drafted) t_drafted = globaltimer_ns();
+        if (!ld_relaxed_u32(&S->closing)) {
+            const unsigned long long tail = ld_acquire_sys_u64(&a.H->tail);
+            const unsigned head = ld_relaxed_u32(&S->head);
+            if (head < tail) {
+                const unsigned long long old = atomicAnd(&S->idle, ~mine);
+                if (!(old & mine)) {  // drafted meanwhile: the mailbox gets the command
+                    if (!t_drafted) t_drafted = globaltimer_ns();
+                    continue;
+                }
+                if (atomicCAS(&S->head, head, head + 1) == head) {
+                    atomicMax(&S->last_busy, globaltimer_ns());
+                    if (!lead_team(a, lane, head, tail)) atomicOr(&S->idle, mine);
+                } else {
+                    atomicOr(&S->idle, mine);  // another lane claimed it first
+                }
+                sleep_ns = 32;
                 continue;
             }
-            if (atomicCAS(&S->head, head, head + 1) == head) {
-                if (!lead_team(a, lane, head, tail)) atomicOr(&S->idle, mine);
-            } else {
-                atomicOr(&S->idle, mine);  // another lane claimed it first
+            const unsigned long long now = globaltimer_ns();
+            const unsigned long long last = max(ld_relaxed_u64(&S->last_busy), t_start);
+            const bool all_idle = ld_relaxed_u64(&S->idle) == a.all_lanes;
+            if (!ld_acquire_sys_u32(&a.H->stop) && !(all_idle && now - last > a.idle_ns)) {
+                __nanosleep(sleep_ns);
+                sleep_ns = min(sleep_ns * 2, 1024u);
+                continue;
             }
-            sleep_ns = 32;
-            continue;
+            atomicExch(&S->closing, 1u);
         }
-        const unsigned long long now = globaltimer_ns();
-        if (ld_acquire_sys_u32(&a.H->stop) || now - t_idle > a.idle_ns) {
+        {
             const unsigned long long old = atomicAnd(&S->idle, ~mine);
             if (old & mine) {  // out of the idle set: nobody can draft this lane now
                 ResLaneBox &b = S->box[lane];
@@ -334,10 +352,8 @@ __device__ void lane_leader_idle(const ResArgs &a, unsigned lane, unsigned seen,
                 return;
             }
             if (!t_drafted) t_drafted = globaltimer_ns();
-            continue;  // drafted
+            continue;  // drafted before the kernel began to close: run that job first
         }
-        __nanosleep(sleep_ns);
-        sleep_ns = min(sleep_ns * 2, 1024u);
     }
 }
 
@@ -358,18 +374,20 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) serve_resident(ResArgs a)
     // Mailboxes start at 0 in every launch (the host clears them), so a
     // command posted before this CTA started is still seen.
     unsigned seen = 0;
-    unsigned long long t_idle = 0;
-    if (threadIdx.x == 0) t_idle = globaltimer_ns();
+    unsigned long long t_start = 0;
+    if (threadIdx.x == 0) t_start = globaltimer_ns();
     for (;;) {
         if (threadIdx.x == 0) {
-            if (r == 0) lane_leader_idle(a, lane, seen, t_idle);
-            // Wait for the lane's command (bounded: the lane's first CTA
-            // posts one within its idle limit).
+            if (r == 0) lane_leader_idle(a, lane, seen, t_start);
+            // Wait for the lane's command.  Bounded: while the device is
+            // busy anywhere, or within idle_ns after, the lane's first CTA
+            // posts a command (a job or kCmdExit).
             const unsigned long long t0 = globaltimer_ns();
             unsigned sleep_ns = 32;
             unsigned s = ld_acquire_u32(&S->box[lane].seq);
             while (s == seen) {
-                if (globaltimer_ns() - t0 > a.idle_ns + a.timeout_ns) break;
+                const unsigned long long ref = max(t0, ld_relaxed_u64(&S->last_busy));
+                if (globaltimer_ns() - ref > a.idle_ns + a.timeout_ns) break;
                 __nanosleep(sleep_ns);
                 sleep_ns = min(sleep_ns * 2, 512u);
                 s = ld_acquire_u32(&S->box[lane].seq);
@@ -425,8 +443,8 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) serve_resident(ResArgs a)
             }
             atomicAdd(&T.left, 1u);  // after this the block may be reset for the next job
             if (r == 0) {
+                atomicMax(&S->last_busy, globaltimer_ns());
                 atomicOr(&S->idle, 1ull << lane);
-                t_idle = globaltimer_ns();
             }
         }
         __syncthreads();
@@ -486,6 +504,7 @@ struct ResidentServer {
     cudaStream_t stream = nullptr;
     cudaEvent_t ev = nullptr;
     const void *kern = nullptr;
+    unsigned long long all_lanes = 0;  // source of the launch's idle-mask copy
     bool running = false;
     uint64_t launches = 0;
 
@@ -507,8 +526,13 @@ namespace {
 // Launches the resident kernel (mu held).  All lanes start idle.
 gft_status launch_locked(ResidentServer *s)
 {
-    unsigned long long all = s->nlanes >= 64 ? ~0ull : ((1ull << s->nlanes) - 1);
-    GFT_CUDA_TRY(cudaMemcpyAsync(&s->D->idle, &all, sizeof all, cudaMemcpyHostToDevice, s->stream));
+    // idle = every lane, last_busy = 0, closing = 0; head persists.
+    static const unsigned long long zero = 0;
+    const unsigned long long all = s->nlanes >= 64 ? ~0ull : ((1ull << s->nlanes) - 1);
+    s->all_lanes = all;
+    GFT_CUDA_TRY(cudaMemcpyAsync(&s->D->idle, &s->all_lanes, sizeof all, cudaMemcpyHostToDevice, s->stream));
+    GFT_CUDA_TRY(cudaMemcpyAsync(&s->D->last_busy, &zero, sizeof zero, cudaMemcpyHostToDevice, s->stream));
+    GFT_CUDA_TRY(cudaMemsetAsync(&s->D->closing, 0, sizeof(unsigned), s->stream));
     // Mailboxes and control blocks: nothing of an earlier launch is left in them.
     GFT_CUDA_TRY(cudaMemsetAsync(s->D->box, 0, sizeof(s->D->box), s->stream));
     GFT_CUDA_TRY(cudaMemsetAsync(s->D->team, 0, sizeof(s->D->team), s->stream));
@@ -524,6 +548,7 @@ gft_status launch_locked(ResidentServer *s)
     a.arenas = s->arenas;
     a.arena_bytes = s->cfg.lane_arena_bytes;
     a.hub_degree = s->cfg.hub_degree;
+    a.all_lanes = all;
     a.idle_ns = (unsigned long long)s->cfg.idle_exit_us * 1000ull;
     a.timeout_ns = 20000ull * 1000000ull;
     void *args[] = {&a};
