@@ -923,15 +923,21 @@ def bench_msbfs(gft, dev: int, k: int = 256, reps: int = 3, max_levels: int = 16
     }
 
 
-def bench_serve(gft, dev: int, rates=(100, 200, 400, 700, 1000, 1500, 2000, 3000, 5000),
-                p99_targets=(5.0, 10.0, 20.0, 50.0, 100.0), delta: int = 40000) -> dict:
-    """C5: Poisson BFS/SSSP requests (50/50, uniform over the 8 resident
-    graphs, random non-isolated sources) against the continuous-batching
-    server, and against the same engine serving one request at a time with
-    the whole GPU (max_batch 1, one lane, one group of every resident CTA).
-    Both sweep the same offered rates; a sweep stops once the server falls
-    well behind the offered rate.  For each p99 target the result gives the
-    best throughput each server sustained within it."""
+def bench_serve(gft, dev: int, rates=(200, 1000, 3000, 10000, 50000),
+                p99_targets=(10.0, 20.0, 50.0, 100.0, 500.0), delta: int = 40000) -> dict:
+    """C5: Poisson BFS/SSSP requests with random non-isolated sources over
+    resident graphs, at offered rates from 200 to 50,000 requests/s, against
+    - the resident serving kernel (one persistent launch; requests through a
+      mapped ring; teams of lanes drafted on the device, gft_serve resident=1),
+    - the lane server (one launch per lane micro-batch, resident=0), and
+    - the same engine serving one request at a time with the whole GPU
+      (max_batch 1, one lane, one group of every resident CTA).
+    Three mixes: the configured one (50/50 BFS/SSSP over the 8 graphs), a
+    BFS-only one over the same graphs, and 50/50 over the three smallest
+    graphs (road 1024^2, RMAT-18, RMAT-20).  Each sweep offers every rate
+    (arrivals wait for a free output buffer and are counted as throttled);
+    for each p99 target the result gives the best throughput each server
+    sustained within it."""
     import torch
 
     from galoisgpu_b200 import workloads as wl
@@ -944,53 +950,65 @@ def bench_serve(gft, dev: int, rates=(100, 200, 400, 700, 1000, 1500, 2000, 3000
     # Output buffers: each in-flight request owns one; about 1.5 GB per graph.
     pools = [[torch.empty(g.nnodes, dtype=torch.int32, device=f"cuda:{dev}")
               for _ in range(max(4, min(256, int(1.5e9 // (4 * g.nnodes)))))] for g in graphs]
+    torch.cuda.synchronize(dev)
     setup_s = time.time() - t0
     eng = gft.Engine(dev)
+    small = [i for i, sp in enumerate(specs) if sp["nodes"] <= 1 << 20]
 
-    def sweep(srv, tag):
+    def sweep(srv, tag, idx, bfs_fraction):
         out = []
         for r in rates:
-            n = int(min(3000, max(400, r * 1.5)))
-            res = poisson_run(srv, graphs, sources, pools, rate=r, n_requests=n, seed=7, delta=delta)
+            n = int(min(1500, max(300, r * 0.5)))
+            res = poisson_run(srv, [graphs[i] for i in idx], [sources[i] for i in idx], [pools[i] for i in idx],
+                              rate=r, n_requests=n, seed=7, delta=delta, bfs_fraction=bfs_fraction)
             out.append(res)
             log(f"[{tag}] rate {r}: {res['achieved_qps']:.0f} q/s p50 {res['p50_ms']:.2f} ms "
-                f"p99 {res['p99_ms']:.2f} ms width {res['mean_width']:.1f}")
-            if res["achieved_qps"] < 0.7 * r:
-                break
+                f"p99 {res['p99_ms']:.2f} ms width {res['mean_width']:.1f} throttled {res['throttled_arrivals']}")
         return out
-
-    srv = Server(eng)
-    cfg = dict(srv.config)
-    runs = sweep(srv, "serve")
-    srv.close()
-    base = Server(eng, lanes=1, max_batch=1, group_min_nodes=1, group_blocks=10**6)
-    base_runs = sweep(base, "serve one-at-a-time")
-    base.close()
-    eng.close()
-    del pools
-    for g in graphs:
-        g.free()
 
     def best_under(rs, p99):
         ok = [x["achieved_qps"] for x in rs if x["p99_ms"] is not None and x["p99_ms"] <= p99 and x["failures"] == 0]
         return max(ok) if ok else 0.0
 
-    equal = []
-    for t in p99_targets:
-        a, b = best_under(runs, t), best_under(base_runs, t)
-        equal.append({"p99_ms": t, "serving_qps": a, "one_at_a_time_qps": b, "speedup": (a / b) if b else None})
-    return {
-        "graphs": [wl.name(sp) for sp in specs],
-        "nodes_total": sum(sp["nodes"] for sp in specs),
-        "setup_s": setup_s,
-        "config": {k: v for k, v in cfg.items()},
-        "delta": delta,
-        "serving": runs,
-        "one_at_a_time": base_runs,
-        "at_equal_p99": equal,
-        "peak_qps": {"serving": max(x["achieved_qps"] for x in runs),
-                     "one_at_a_time": max(x["achieved_qps"] for x in base_runs)},
+    servers = {
+        "resident": dict(resident=1, lane_blocks=8, lane_arena_bytes=1600 << 20),
+        "lanes": {},
+        "one_at_a_time": dict(lanes=1, max_batch=1, group_min_nodes=1, group_blocks=10**6),
     }
+    mixes = {
+        "mix": (list(range(len(specs))), 0.5, ("resident", "lanes", "one_at_a_time")),
+        "bfs_only": (list(range(len(specs))), 1.0, ("resident", "one_at_a_time")),
+        "small_graphs": (small, 0.5, ("resident", "one_at_a_time")),
+    }
+    result = {"graphs": [wl.name(sp) for sp in specs], "nodes_total": sum(sp["nodes"] for sp in specs),
+              "setup_s": setup_s, "delta": delta, "offered_rates": list(rates)}
+    for mname, (idx, bfs_fraction, names) in mixes.items():
+        runs = {}
+        for sname in names:
+            srv = Server(eng, **servers[sname])
+            runs[sname] = sweep(srv, f"{mname} {sname}", idx, bfs_fraction)
+            srv.close()
+        equal = []
+        for t in p99_targets:
+            base = best_under(runs["one_at_a_time"], t)
+            row = {"p99_ms": t, "one_at_a_time_qps": base}
+            for sname in names:
+                if sname != "one_at_a_time":
+                    q = best_under(runs[sname], t)
+                    row[f"{sname}_qps"] = q
+                    row[f"{sname}_speedup"] = (q / base) if base else None
+            equal.append(row)
+        result[mname] = {
+            "graphs": [wl.name(specs[i]) for i in idx], "bfs_fraction": bfs_fraction, "runs": runs,
+            "at_equal_p99": equal,
+            "peak_qps": {k: max(x["achieved_qps"] for x in v) for k, v in runs.items()},
+        }
+        log(f"[{mname}] peak q/s " + ", ".join(f"{k} {v:.0f}" for k, v in result[mname]["peak_qps"].items()))
+    eng.close()
+    del pools
+    for g in graphs:
+        g.free()
+    return result
 
 
 def _kms_by_source(res) -> dict:
@@ -1379,7 +1397,8 @@ def main(argv=None) -> int:
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("gft", "reference"), default="gft")
     ap.add_argument("--workload",
-                    choices=sorted(WORKLOADS) + sorted(CC_WORKLOADS) + sorted(PR_WORKLOADS) + sorted(MIS_WORKLOADS),
+                    choices=sorted(WORKLOADS) + sorted(CC_WORKLOADS) + sorted(PR_WORKLOADS) + sorted(MIS_WORKLOADS)
+                    + ["serve-8-graphs", "batch-sssp-512", "msbfs-rmat24-256"],
                     default=HEADLINE, help="a traversal workload (the headline by default), or a connected-components, "
                                            "PageRank or maximal-independent-set one")
     ap.add_argument("--no-secondary", action="store_true", help="skip the secondary workloads")
@@ -1392,7 +1411,24 @@ def main(argv=None) -> int:
         return reference_arm(args)
     if args.workload in CC_WORKLOADS or args.workload in PR_WORKLOADS or args.workload in MIS_WORKLOADS:
         return cc_arm(args)
+    if args.workload in ("serve-8-graphs", "batch-sssp-512", "msbfs-rmat24-256"):
+        return many_arm(args)
     return our_arm(args)
+
+
+def many_arm(args) -> int:
+    """One of the many-query workloads (serving, batching, multi-source BFS)
+    alone on one GPU, as a JSON line."""
+    import torch
+
+    import galoisgpu_b200 as gft
+
+    torch.cuda.set_device(0)
+    fn = {"serve-8-graphs": bench_serve, "batch-sssp-512": bench_batch, "msbfs-rmat24-256": bench_msbfs}[args.workload]
+    r = fn(gft, 0)
+    print(json.dumps({"workload": args.workload, "n_gpus": 1, "data": "synthetic: seeded graphs generated on the device",
+                      **r}), flush=True)
+    return 0
 
 
 def cc_arm(args) -> int:

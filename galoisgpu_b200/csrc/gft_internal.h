@@ -111,7 +111,7 @@ struct BatchJob {
     uint32_t vec_ok;
     uint32_t uniform;  // max degree <= kUniformDegree: static chunks
     uint32_t dir_opt;  // BFS on a graph marked symmetric: direction-optimising
-    uint32_t pad2;
+    uint32_t min_lanes;  // resident serving: lanes the job asks for at least (0 or 1: no minimum)
     uint32_t status, error_where, levels, iterations;
     unsigned long long edges;
     unsigned long long t_start, t_end;  // %globaltimer, ns

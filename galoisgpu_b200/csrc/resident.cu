@@ -64,6 +64,7 @@
 namespace gft {
 
 constexpr unsigned kResMaxLanes = 64;  // one bit per lane in the idle mask
+constexpr unsigned long long kGatherNs = 3000000;  // longest wait of a large job for its minimum width
 constexpr unsigned kCmdRun = 1, kCmdExit = 2;
 
 struct alignas(128) ResLaneBox {
@@ -233,28 +234,11 @@ __device__ bool lead_team(const ResArgs &a, unsigned lane, unsigned long long h,
 {
     ResDev *S = a.S;
     const unsigned long long mine = 1ull << lane;
-    // Width: the idle lanes shared among the jobs still waiting.
-    const unsigned long long snap = ld_relaxed_u64(&S->idle) & ~mine;
-    const unsigned long long waiting = tail > h + 1 ? tail - (h + 1) : 0;
-    const unsigned long long idle_lanes = (unsigned long long)__popcll(snap) + 1;  // with this lane
-    unsigned want = (unsigned)(idle_lanes / (waiting + 1));
-    want = max(1u, min(want, a.max_team_lanes));
-    unsigned long long pick = 0, rest = snap;
-    for (unsigned k = 1; k < want && rest; k++) {
-        const unsigned long long low = rest & (~rest + 1);
-        pick |= low;
-        rest &= rest - 1;
-    }
-    unsigned long long got = 0;
-    if (pick) got = atomicAnd(&S->idle, ~pick) & pick;
-    const unsigned team_lanes = 1 + __popcll(got);
-
     ResTeam &T = S->team[lane];
     // The control block is free once every CTA of its last job left it.
     const unsigned long long t0 = globaltimer_ns();
     while (ld_acquire_u32(&T.left) != __ldcg(&T.members)) {
         if (globaltimer_ns() - t0 > a.timeout_ns) {
-            if (got) atomicOr(&S->idle, got);
             // The job cannot run here: report it.
             ResDone &d = a.done[h % a.ring_size];
             d.status = GFT_ERR_TIMEOUT;
@@ -266,12 +250,53 @@ __device__ bool lead_team(const ResArgs &a, unsigned lane, unsigned long long h,
             return false;
         }
     }
+    load_ring_job(&T.job, a.ring + h % a.ring_size);  // from mapped host memory
+    // Width: the idle lanes shared among the jobs still waiting, but at least
+    // the job's own minimum (a large graph runs several times slower per
+    // query on a narrow team than alone), as far as idle lanes allow.
+    const unsigned long long snap = ld_relaxed_u64(&S->idle) & ~mine;
+    const unsigned long long waiting = tail > h + 1 ? tail - (h + 1) : 0;
+    const unsigned long long idle_lanes = (unsigned long long)__popcll(snap) + 1;  // with this lane
+    unsigned want = (unsigned)(idle_lanes / (waiting + 1));
+    want = max(want, T.job.min_lanes);
+    want = max(1u, min(want, a.max_team_lanes));
+    unsigned long long pick = 0, rest = snap;
+    for (unsigned k = 1; k < want && rest; k++) {
+        const unsigned long long low = rest & (~rest + 1);
+        pick |= low;
+        rest &= rest - 1;
+    }
+    unsigned long long got = 0;
+    if (pick) got = atomicAnd(&S->idle, ~pick) & pick;
+    // A large job that found too few idle lanes gathers more as other teams
+    // finish, for at most kGatherNs: on one or two lanes it would run several
+    // times longer than on its minimum.
+    const unsigned need = min(max(T.job.min_lanes, 1u), a.max_team_lanes);
+    if ((unsigned)__popcll(got) + 1 < need) {
+        const unsigned long long tg = globaltimer_ns();
+        unsigned sleep_ns = 64;
+        while ((unsigned)__popcll(got) + 1 < need && globaltimer_ns() - tg < kGatherNs) {
+            unsigned long long more = ld_relaxed_u64(&S->idle) & ~mine & ~got;
+            unsigned long long take = 0;
+            for (unsigned k = __popcll(got) + 1; k < need && more; k++) {
+                const unsigned long long low = more & (~more + 1);
+                take |= low;
+                more &= more - 1;
+            }
+            if (take) got |= atomicAnd(&S->idle, ~take) & take;
+            else {
+                __nanosleep(sleep_ns);
+                sleep_ns = min(sleep_ns * 2, 1024u);
+            }
+        }
+    }
+    const unsigned team_lanes = 1 + __popcll(got);
+
     reset_team_ctl(&T.ctl);
     T.left = 0;
     T.members = team_lanes * a.lane_ctas;
     T.index = (unsigned)h;
     T.t_claim = globaltimer_ns();
-    load_ring_job(&T.job, a.ring + h % a.ring_size);  // from mapped host memory
     __threadfence();
     // Commands: this lane is rank 0, the drafted lanes follow in lane order.
     unsigned rank = 0;
@@ -476,6 +501,12 @@ extern "C" GFT_API int gft_debug_resident_trace(unsigned long long *host, int ma
 #endif
 
 namespace {
+
+// Edges per lane of 8 CTAs up to which a team of that many lanes served a
+// query about as efficiently as the whole device did (serving graphs on a
+// B200: 2-11x more queries side by side up to 16 M edges, 0.5-0.7x on
+// 64 M-edge graphs run on one or two lanes).
+constexpr uint64_t kLaneEdges = 8ull << 20;
 
 using Clock = std::chrono::steady_clock;
 double now_ms() { return std::chrono::duration<double, std::milli>(Clock::now().time_since_epoch()).count(); }
@@ -714,6 +745,10 @@ gft_status resident_enqueue(ResidentServer *s, const gft_query &q, size_t scratc
     BatchJob &j = s->h_ring[idx % s->ring];
     fill_batch_job(j, q, s->cfg.hub_degree);
     j.scratch = 0;  // at the start of the team leader's arena
+    // About kLaneEdges edges per lane: below that a narrow team serves the
+    // query as efficiently as the whole device; above, it slows down.
+    const uint64_t e = q.graph->g.nedges;
+    j.min_lanes = (uint32_t)std::min<uint64_t>(s->nlanes, std::max<uint64_t>(1, (e + kLaneEdges - 1) / kLaneEdges));
     sl.busy = true;
     sl.ticket = s->next_ticket++;
     sl.t_arrive = now_ms();

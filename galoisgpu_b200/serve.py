@@ -93,18 +93,23 @@ def poisson_run(server: Server, graphs: list[DeviceGraph], sources: list[list[in
     free = [list(range(len(p))) for p in pools]
     lock = threading.Lock()
     busy = {}  # ticket -> (graph index, buffer index)
-    lat, qms, lanes, bsz, width = [], [], {}, [], []
+    lat, qms, lanes, bsz, width, slow = [], [], {}, [], [], []
     failures = 0
     done = [0]
     stop = [False]
 
     def collector():
         nonlocal failures
+        last = time.perf_counter()
         while not stop[0] or done[0] < n_requests:
+            if time.perf_counter() - last > 300:
+                raise TimeoutError(f"poisson_run: no completion for 300 s ({done[0]} of {n_requests} done)")
             for c in server.poll(4096, 2000):
+                last = time.perf_counter()
                 with lock:
-                    gi, bi = busy.pop(c["ticket"])
+                    gi, bi, app = busy.pop(c["ticket"])
                     free[gi].append(bi)
+                slow.append((c["latency_ms"], gi, app, c["width"], c["queue_ms"]))
                 if c["status"] != 0:
                     failures += 1
                 lat.append(c["latency_ms"])
@@ -147,7 +152,7 @@ def poisson_run(server: Server, graphs: list[DeviceGraph], sources: list[list[in
         throttled += waited
         with lock:  # the collector may see the completion before enqueue returns
             t = server.enqueue(graphs[gi], app, src, pools[gi][bi], delta=delta)
-            busy[t] = (gi, bi)
+            busy[t] = (gi, bi, app)
     offered_s = time.perf_counter() - t0
     stop[0] = True
     th.join(timeout=600)
@@ -167,4 +172,6 @@ def poisson_run(server: Server, graphs: list[DeviceGraph], sources: list[list[in
         "lanes": lanes,
         "throttled_arrivals": throttled,
         "failures": failures,
+        # The slowest requests: (latency ms, graph index, app, team width, queue ms).
+        "slowest": sorted(slow, reverse=True)[:5],
     }
