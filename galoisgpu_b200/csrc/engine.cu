@@ -63,6 +63,24 @@ __global__ void first_bad_edge(const uint32_t *__restrict__ dst, uint32_t m, uin
         }
 }
 
+// One 16-byte slot per vertex: its destinations, or kBfsSlotWide.
+__global__ void build_bfs_slots(const uint32_t *__restrict__ row_start, const uint32_t *__restrict__ dst, uint32_t n,
+                                uint4 *__restrict__ slots)
+{
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+        const uint32_t s = row_start[v], d = row_start[v + 1] - s;
+        uint4 x = make_uint4(kBfsSlotNone, kBfsSlotNone, kBfsSlotNone, kBfsSlotNone);
+        if (d > 4) x.x = kBfsSlotWide;
+        else {
+            if (d > 0) x.x = dst[s];
+            if (d > 1) x.y = dst[s + 1];
+            if (d > 2) x.z = dst[s + 2];
+            if (d > 3) x.w = dst[s + 3];
+        }
+        slots[v] = x;
+    }
+}
+
 __global__ void interleave_edges(const uint32_t *__restrict__ dst, const int32_t *__restrict__ w, uint32_t m,
                                  uint2 *__restrict__ out)
 {
@@ -93,6 +111,31 @@ gft_status ensure_edge_pairs(gft_graph *g, cudaStream_t stream)
         return fail(GFT_ERR_CUDA, "interleaving edges: %s", cudaGetErrorString(err));
     }
     G.edge_dw = p;  // complete before any query can see it
+    return GFT_OK;
+}
+
+gft_status ensure_bfs_slots(gft_graph *g, cudaStream_t stream)
+{
+    std::lock_guard<std::mutex> lk(g->pair_mu);
+    DeviceGraph &G = g->g;
+    if (G.bfs_slots || !G.nnodes) return GFT_OK;
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(stream, &cap) != cudaSuccess || cap != cudaStreamCaptureStatusNone) return GFT_OK;
+    DeviceScope device_scope(G.device);
+    GFT_CUDA_TRY(device_scope.err);
+    uint4 *p = nullptr;
+    if (cudaMalloc(&p, (size_t)G.nnodes * sizeof(uint4)) != cudaSuccess) {
+        cudaGetLastError();  // no room: the BFS reads the CSR
+        return GFT_OK;
+    }
+    dev::build_bfs_slots<<<148 * 4, 256, 0, stream>>>(G.row_start, G.edge_dst, G.nnodes, p);
+    cudaError_t err = cudaGetLastError();
+    if (err == cudaSuccess) err = cudaStreamSynchronize(stream);
+    if (err != cudaSuccess) {
+        cudaFree(p);
+        return fail(GFT_ERR_CUDA, "building BFS slots: %s", cudaGetErrorString(err));
+    }
+    G.bfs_slots = p;  // complete before any query can see it
     return GFT_OK;
 }
 
@@ -368,9 +411,10 @@ void gft_graph_free(gft_graph *g)
         if (g->g.edge_dst) cudaFree(g->g.edge_dst);
         if (g->g.edge_data) cudaFree(g->g.edge_data);
     }
-    if (g->g.edge_dw) {
+    if (g->g.edge_dw || g->g.bfs_slots) {
         DeviceScope device_scope(g->g.device);
-        cudaFree(g->g.edge_dw);
+        if (g->g.edge_dw) cudaFree(g->g.edge_dw);
+        if (g->g.bfs_slots) cudaFree(g->g.bfs_slots);
     }
     delete g;
 }

@@ -31,6 +31,7 @@ struct TravParams {
     const uint32_t *__restrict__ edge_dst;
     const int32_t *__restrict__ edge_data;  // SSSP; NULL = every weight 0
     const uint2 *__restrict__ edge_dw;      // SSSP: (edge_dst, edge_data) interleaved, or NULL
+    const uint4 *__restrict__ bfs_slots;    // one-CTA thread-per-vertex BFS: 16-byte slot per vertex, or NULL
     uint32_t nnodes;
     uint32_t src;
     int32_t *out;       // level / dist

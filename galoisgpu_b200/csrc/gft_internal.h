@@ -48,7 +48,15 @@ struct DeviceGraph {
     // SSSP query and owned by the graph even when the arrays above are
     // wrapped; NULL until then.
     uint2 *edge_dw = nullptr;
+    // Small low-degree graphs (the one-CTA thread-per-vertex BFS): one
+    // 16-byte slot per vertex with its up to 4 destinations (kBfsSlotNone
+    // after them), or kBfsSlotWide first for a vertex of more edges.  Built
+    // on the first such BFS, owned by the graph; NULL until then.
+    uint4 *bfs_slots = nullptr;
 };
+
+constexpr uint32_t kBfsSlotNone = 0xFFFFFFFFu;  // never a destination: ids are < nnodes <= 2^32 - 2
+constexpr uint32_t kBfsSlotWide = 0xFFFFFFFEu;
 
 // Lazily grown device allocation owned by an engine.
 struct Scratch {
@@ -176,6 +184,9 @@ struct DeviceScope {
 // there yet, and waits for it; on an allocation failure, or while `stream`
 // is being captured, the graph keeps the separate arrays only.
 gft_status ensure_edge_pairs(gft_graph *g, cudaStream_t stream);
+// Builds g->g.bfs_slots on `stream` (not under stream capture; no room:
+// left NULL, and the BFS reads the CSR).
+gft_status ensure_bfs_slots(gft_graph *g, cudaStream_t stream);
 gft_status graph_degree_stats(DeviceGraph &G, cudaStream_t stream);
 // Resident-kernel serving (resident.cu), behind gft_serve_* when
 // gft_serve_config.resident is set.

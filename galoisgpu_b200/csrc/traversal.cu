@@ -126,15 +126,26 @@ __global__ void __launch_bounds__(kCtaBlock, 1) bfs_single_cta(TravParams p)
 // four at a time (read through L1: a level's rows sit next to the previous
 // level's on these graphs).  The visited bitmap and the first kLaneQueueHead entries of
 // both frontier queues live in shared memory; a queue's later entries go to
-// the engine's global queue at the same index.  A level is: row pair and
-// edge loads, probes and claims in shared memory, one shared atomic per warp
-// step for the appends, one __syncthreads.  Always top-down: levels are the
-// same in either direction, and these graphs' frontiers stay small.
+// the engine's global queue at the same index.  With the graph's BFS slots
+// (16 bytes per vertex holding its up to 4 destinations), a vertex's edges
+// are one load instead of a row lookup and then an edge load, and a thread
+// that claims a vertex prefetches its slot into L1 for the next level, so
+// a level waits for about one cache hit instead of two L2 round trips; a
+// vertex of more than 4 edges is read through the CSR.  A level is: slot
+// (or row pair and edge) loads, claims in shared memory, one shared atomic
+// per warp step for the appends, one __syncthreads.  Always top-down: levels
+// are the same in either direction, and these graphs' frontiers stay small.
 // ---------------------------------------------------------------------------
-constexpr uint32_t kLaneQueueHead = 16384;
+constexpr uint32_t kLaneQueueHead = 8192;
+
+__device__ __forceinline__ void prefetch_l1(const void *p)
+{
+    asm volatile("prefetch.global.L1 [%0];" ::"l"(p));
+}
 constexpr size_t kLaneSmemBytes = (kCtaLocalBitsNodes / 32 + 2 * (size_t)kLaneQueueHead) * 4;
 
-__global__ void __launch_bounds__(kCtaBlock, 1) bfs_cta_lanes(TravParams p)
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK, 1) bfs_cta_lanes(TravParams p)
 {
     extern __shared__ __align__(16) uint32_t s_lane[];
     uint32_t *bits = s_lane;
@@ -143,11 +154,11 @@ __global__ void __launch_bounds__(kCtaBlock, 1) bfs_cta_lanes(TravParams p)
     __shared__ unsigned s_err;
     const unsigned tid = threadIdx.x, lane = tid & 31;
     const uint32_t n = p.nnodes, nwords = (n + 31) >> 5;
-    for (uint32_t v = tid; v < n; v += kCtaBlock) {
+    for (uint32_t v = tid; v < n; v += BLOCK) {
         p.out[v] = v == p.src ? 0 : (int32_t)kInf;
         if (p.parent) p.parent[v] = v == p.src ? p.src : GFT_NO_PARENT;
     }
-    for (uint32_t w = tid; w < nwords; w += kCtaBlock) bits[w] = w == (p.src >> 5) ? 1u << (p.src & 31) : 0u;
+    for (uint32_t w = tid; w < nwords; w += BLOCK) bits[w] = w == (p.src >> 5) ? 1u << (p.src & 31) : 0u;
     if (tid == 0) {
         head0[0] = p.src;
         s_len[0] = 1;
@@ -157,6 +168,7 @@ __global__ void __launch_bounds__(kCtaBlock, 1) bfs_cta_lanes(TravParams p)
     }
     __syncthreads();
 
+    const uint4 *__restrict__ slots = p.bfs_slots;
     unsigned long long edges = 0, claimed = 0;
     unsigned L = 0;
     for (;;) {
@@ -171,19 +183,36 @@ __global__ void __launch_bounds__(kCtaBlock, 1) bfs_cta_lanes(TravParams p)
         const uint32_t *in_head = (L & 1) ? head1 : head0, *in_tail = sel2(p.q, L);
         uint32_t *out_head = (L & 1) ? head0 : head1, *out_tail = sel2(p.q, L + 1);
         const int32_t next_level = (int32_t)L + 1;
-        for (unsigned base = tid - lane; base < n_in; base += kCtaBlock) {  // warp-uniform trip count
+        for (unsigned base = tid - lane; base < n_in; base += BLOCK) {  // warp-uniform trip count
             const unsigned i = base + lane;
             uint32_t u = 0, s = 0, deg = 0;
+            uint4 sl = make_uint4(kBfsSlotNone, kBfsSlotNone, kBfsSlotNone, kBfsSlotNone);
+            bool from_slot = false;
             if (i < n_in) {
                 u = i < kLaneQueueHead ? in_head[i] : __ldcg(in_tail + i);
-                s = __ldg(p.row_start + u);
-                deg = __ldg(p.row_start + u + 1) - s;
+                if (slots) {
+                    sl = __ldg(slots + u);
+                    from_slot = sl.x != kBfsSlotWide;
+                    deg = (sl.x != kBfsSlotNone) + (sl.y != kBfsSlotNone) + (sl.z != kBfsSlotNone) +
+                          (sl.w != kBfsSlotNone);
+                }
+                if (!from_slot) {
+                    s = __ldg(p.row_start + u);
+                    deg = __ldg(p.row_start + u + 1) - s;
+                }
             }
             const unsigned max_deg = __reduce_max_sync(kFull, deg);
             for (unsigned j = 0; j < max_deg; j += 4) {
                 uint32_t v[4];
+                if (from_slot) {  // deg <= 4: only j == 0
+                    v[0] = sl.x;
+                    v[1] = sl.y;
+                    v[2] = sl.z;
+                    v[3] = sl.w;
+                } else {
 #pragma unroll
-                for (int k = 0; k < 4; k++) v[k] = j + k < deg ? __ldg(p.edge_dst + s + j + k) : 0u;
+                    for (int k = 0; k < 4; k++) v[k] = j + k < deg ? __ldg(p.edge_dst + s + j + k) : 0u;
+                }
                 // The four claims go out together, with no probe first: a
                 // shared-memory atomic costs about what a load does, and
                 // this keeps one shared round trip per step (road 362^2:
@@ -225,6 +254,7 @@ __global__ void __launch_bounds__(kCtaBlock, 1) bfs_cta_lanes(TravParams p)
                             atomicCAS(&s_err, 0u, (unsigned)GFT_ERR_OVERFLOW);
                         p.out[v[k]] = next_level;
                         if (p.parent) p.parent[v[k]] = u;
+                        if (slots) prefetch_l1(slots + v[k]);
                         claimed++;
                     }
                     at += __popc(mask[k]);
@@ -243,6 +273,29 @@ __global__ void __launch_bounds__(kCtaBlock, 1) bfs_cta_lanes(TravParams p)
         p.ctl->iterations = L + 1;  // barriers, as the general kernel counts them
         if (s_err) p.ctl->error = s_err;
     }
+}
+
+#ifndef GFT_LANES_BLOCK
+#define GFT_LANES_BLOCK 0  // 0: chosen from the vertex count
+#endif
+__host__ __forceinline__ int lanes_block_for(uint32_t nnodes)
+{
+    if (GFT_LANES_BLOCK) return GFT_LANES_BLOCK;
+    // Measured per query: the 256^2 grid (frontiers <= 256) runs in
+    // 0.60 / 0.62 / 0.69 ms at 256 / 512 / 1024 threads, the 362^2 road
+    // graph (random source, frontiers of 700 and more) in 0.75 / 0.50 /
+    // 0.42 ms.  Graphs here have at most kCtaLocalBitsNodes vertices.
+    return nnodes <= (1u << 16) ? 256 : 1024;
+}
+__host__ inline const void *lanes_kernel_for(int block)
+{
+    return block <= 256 ? (const void *)bfs_cta_lanes<256>
+                        : block <= 512 ? (const void *)bfs_cta_lanes<512> : (const void *)bfs_cta_lanes<1024>;
+}
+__host__ inline bool is_lanes_kernel(const void *k)
+{
+    return k == (const void *)bfs_cta_lanes<256> || k == (const void *)bfs_cta_lanes<512> ||
+           k == (const void *)bfs_cta_lanes<1024>;
 }
 
 __global__ void __launch_bounds__(kCtaBlock, 1) sssp_single_cta(TravParams p)
@@ -448,8 +501,14 @@ gft_status run_traversal(bool is_sssp, gft_engine *e, const gft_graph *g, uint32
             kern = (const void *)dev::sssp_single_cta;
         } else if (G.nnodes <= dev::kCtaLocalBitsNodes && G.max_degree <= kUniformDegree) {
             // Thread per frontier vertex, bitmap and queue heads in shared memory.
-            kern = (const void *)dev::bfs_cta_lanes;
+            // A level costs about the instructions its warps issue, and the
+            // idle ones issue too: size the CTA to the frontiers, which on
+            // these graphs stay near the square root of the vertex count.
+            const int lanes_block = dev::lanes_block_for(G.nnodes);
+            shape.block_threads = lanes_block;
+            kern = dev::lanes_kernel_for(lanes_block);
             dyn_smem = dev::kLaneSmemBytes;
+            if (!G.wrapped) GFT_TRY(ensure_bfs_slots(const_cast<gft_graph *>(g), stream));
             GFT_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn_smem));
         } else {
             kern = G.nnodes <= dev::kCtaLocalBitsNodes ? (const void *)dev::bfs_single_cta<true>
@@ -490,6 +549,7 @@ gft_status run_traversal(bool is_sssp, gft_engine *e, const gft_graph *g, uint32
     p.edge_dst = G.edge_dst;
     p.edge_data = G.edge_data;
     p.edge_dw = is_sssp ? G.edge_dw : nullptr;
+    p.bfs_slots = dev::is_lanes_kernel(kern) ? G.bfs_slots : nullptr;
     p.nnodes = n;
     p.src = src;
     p.out = d_out;
