@@ -63,7 +63,8 @@ __global__ void first_bad_edge(const uint32_t *__restrict__ dst, uint32_t m, uin
         }
 }
 
-// One 16-byte slot per vertex: its destinations, or kBfsSlotWide.
+// One 16-byte slot per vertex: its destinations, or kBfsSlotWide for a
+// vertex of more than 4 edges or of an edge leaving the graph.
 __global__ void build_bfs_slots(const uint32_t *__restrict__ row_start, const uint32_t *__restrict__ dst, uint32_t n,
                                 uint4 *__restrict__ slots)
 {
@@ -76,6 +77,10 @@ __global__ void build_bfs_slots(const uint32_t *__restrict__ row_start, const ui
             if (d > 1) x.y = dst[s + 1];
             if (d > 2) x.z = dst[s + 2];
             if (d > 3) x.w = dst[s + 3];
+            // A destination outside the graph sends the vertex through the
+            // CSR, whose reader reports it; slot destinations are in range.
+            if ((d > 0 && x.x >= n) || (d > 1 && x.y >= n) || (d > 2 && x.z >= n) || (d > 3 && x.w >= n))
+                x = make_uint4(kBfsSlotWide, kBfsSlotNone, kBfsSlotNone, kBfsSlotNone);
         }
         slots[v] = x;
     }

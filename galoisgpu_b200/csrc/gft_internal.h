@@ -50,7 +50,8 @@ struct DeviceGraph {
     uint2 *edge_dw = nullptr;
     // Small low-degree graphs (the one-CTA thread-per-vertex BFS): one
     // 16-byte slot per vertex with its up to 4 destinations (kBfsSlotNone
-    // after them), or kBfsSlotWide first for a vertex of more edges.  Built
+    // after them), or kBfsSlotWide first for a vertex of more edges or of
+    // a destination outside the graph (read through the CSR).  Built
     // on the first such BFS, owned by the graph; NULL until then.
     uint4 *bfs_slots = nullptr;
 };

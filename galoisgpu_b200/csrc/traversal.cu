@@ -122,27 +122,74 @@ __global__ void __launch_bounds__(kCtaBlock, 1) bfs_single_cta(TravParams p)
 // a few hundred vertices, so a level costs its critical path, and the
 // general kernel's balancing (prefix sums and shuffle searches over the
 // warp's edges, per-warp queue buffers) costs more than the few edges it
-// balances.  Here a thread walks its vertex's at most kUniformDegree edges
-// four at a time (read through L1: a level's rows sit next to the previous
-// level's on these graphs).  The visited bitmap and the first kLaneQueueHead entries of
-// both frontier queues live in shared memory; a queue's later entries go to
-// the engine's global queue at the same index.  With the graph's BFS slots
-// (16 bytes per vertex holding its up to 4 destinations), a vertex's edges
-// are one load instead of a row lookup and then an edge load, and a thread
-// that claims a vertex prefetches its slot into L1 for the next level, so
-// a level waits for about one cache hit instead of two L2 round trips; a
-// vertex of more than 4 edges is read through the CSR.  A level is: slot
-// (or row pair and edge) loads, claims in shared memory, one shared atomic
-// per warp step for the appends, one __syncthreads.  Always top-down: levels
-// are the same in either direction, and these graphs' frontiers stay small.
+// balances.  The visited bitmap and the first kLaneQueueHead entries of both
+// frontier queues live in shared memory; a queue's later entries go to the
+// engine's global queue at the same index.  With the graph's BFS slots (16
+// bytes per vertex holding its up to 4 destinations, all inside the graph),
+// a vertex's edges are one load instead of a row lookup and then an edge
+// load, and its four claims go out with no range check; a vertex of more
+// edges (or any vertex of a graph without slots) is walked through the CSR
+// four edges at a time.  A level is: slot loads, claims in shared memory,
+// one shared atomic per warp step for the appends, one __syncthreads.  The
+// level costs about the instructions of its longest warp, so the common
+// path keeps them few: edges are counted per vertex, and a warp step whose
+// appends all fit the shared queue head stores them with no per-vertex
+// check.  Always top-down: levels are the same in either direction, and
+// these graphs' frontiers stay small.
 // ---------------------------------------------------------------------------
 constexpr uint32_t kLaneQueueHead = 8192;
-
-__device__ __forceinline__ void prefetch_l1(const void *p)
-{
-    asm volatile("prefetch.global.L1 [%0];" ::"l"(p));
-}
 constexpr size_t kLaneSmemBytes = (kCtaLocalBitsNodes / 32 + 2 * (size_t)kLaneQueueHead) * 4;
+
+// One warp step's appends: claimed destinations v[k] (mine[k]) of frontier
+// vertex u go to the next frontier and get their level.  Each vertex is
+// claimed once, so a level appends fewer than qcap = nnodes entries.
+__device__ __forceinline__ void lanes_append(const TravParams &p, const bool (&mine)[4], const uint32_t (&v)[4],
+                                             uint32_t u, unsigned *len_next, uint32_t *out_head,
+                                             uint32_t *out_tail, int32_t level, unsigned *err, unsigned lane,
+                                             unsigned long long &claimed)
+{
+    unsigned mask[4], total = 0;
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        mask[k] = __ballot_sync(kFull, mine[k]);
+        total += __popc(mask[k]);
+    }
+    if (total == 0) return;  // warp uniform
+    unsigned at = 0;
+    if (lane == 0) {
+        at = atomicAdd(len_next, total);
+        claimed += total;
+    }
+    at = __shfl_sync(kFull, at, 0);
+    const unsigned lt = lanemask_lt();
+    if (at + total <= kLaneQueueHead) {  // warp uniform
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            if (mine[k]) {
+                out_head[at + __popc(mask[k] & lt)] = v[k];
+                p.out[v[k]] = level;
+                if (p.parent) p.parent[v[k]] = u;
+            }
+            at += __popc(mask[k]);
+        }
+        return;
+    }
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        if (mine[k]) {
+            const unsigned slot = at + __popc(mask[k] & lt);
+            if (slot < kLaneQueueHead)
+                out_head[slot] = v[k];
+            else if (slot < p.qcap)
+                out_tail[slot] = v[k];
+            else
+                atomicCAS(err, 0u, (unsigned)GFT_ERR_OVERFLOW);
+            p.out[v[k]] = level;
+            if (p.parent) p.parent[v[k]] = u;
+        }
+        at += __popc(mask[k]);
+    }
+}
 
 template <int BLOCK>
 __global__ void __launch_bounds__(BLOCK, 1) bfs_cta_lanes(TravParams p)
@@ -169,6 +216,7 @@ __global__ void __launch_bounds__(BLOCK, 1) bfs_cta_lanes(TravParams p)
     __syncthreads();
 
     const uint4 *__restrict__ slots = p.bfs_slots;
+    const uint4 none = make_uint4(kBfsSlotNone, kBfsSlotNone, kBfsSlotNone, kBfsSlotNone);
     unsigned long long edges = 0, claimed = 0;
     unsigned L = 0;
     for (;;) {
@@ -185,79 +233,57 @@ __global__ void __launch_bounds__(BLOCK, 1) bfs_cta_lanes(TravParams p)
         const int32_t next_level = (int32_t)L + 1;
         for (unsigned base = tid - lane; base < n_in; base += BLOCK) {  // warp-uniform trip count
             const unsigned i = base + lane;
-            uint32_t u = 0, s = 0, deg = 0;
-            uint4 sl = make_uint4(kBfsSlotNone, kBfsSlotNone, kBfsSlotNone, kBfsSlotNone);
-            bool from_slot = false;
+            uint32_t u = 0;
+            uint4 sl = none;
+            bool csr = false;
             if (i < n_in) {
                 u = i < kLaneQueueHead ? in_head[i] : __ldcg(in_tail + i);
-                if (slots) {
-                    sl = __ldg(slots + u);
-                    from_slot = sl.x != kBfsSlotWide;
-                    deg = (sl.x != kBfsSlotNone) + (sl.y != kBfsSlotNone) + (sl.z != kBfsSlotNone) +
-                          (sl.w != kBfsSlotNone);
-                }
-                if (!from_slot) {
-                    s = __ldg(p.row_start + u);
-                    deg = __ldg(p.row_start + u + 1) - s;
-                }
+                if (slots) sl = __ldg(slots + u);
+                csr = !slots || sl.x == kBfsSlotWide;
+                if (csr) sl = none;
             }
-            const unsigned max_deg = __reduce_max_sync(kFull, deg);
-            for (unsigned j = 0; j < max_deg; j += 4) {
-                uint32_t v[4];
-                if (from_slot) {  // deg <= 4: only j == 0
-                    v[0] = sl.x;
-                    v[1] = sl.y;
-                    v[2] = sl.z;
-                    v[3] = sl.w;
-                } else {
-#pragma unroll
-                    for (int k = 0; k < 4; k++) v[k] = j + k < deg ? __ldg(p.edge_dst + s + j + k) : 0u;
-                }
-                // The four claims go out together, with no probe first: a
-                // shared-memory atomic costs about what a load does, and
-                // this keeps one shared round trip per step (road 362^2:
-                // 5% faster than probe-then-claim per edge).
+            // Slot destinations.  The four claims go out together, with no
+            // probe first: a shared-memory atomic costs about what a load
+            // does, and this keeps one shared round trip per step.
+            {
+                const uint32_t v[4] = {sl.x, sl.y, sl.z, sl.w};
                 bool mine[4];
 #pragma unroll
                 for (int k = 0; k < 4; k++) {
-                    mine[k] = false;
-                    if (j + k < deg) {
-                        edges++;
-                        const uint32_t b = 1u << (v[k] & 31);
-                        if (v[k] < n)
-                            mine[k] = !(atomicOr(bits + (v[k] >> 5), b) & b);
-                        else
-                            atomicCAS(&s_err, 0u, (unsigned)GFT_ERR_FORMAT);
-                    }
+                    const bool valid = v[k] != kBfsSlotNone;
+                    const uint32_t b = 1u << (v[k] & 31);
+                    uint32_t old = b;
+                    if (valid) old = atomicOr(bits + (v[k] >> 5), b);
+                    mine[k] = !(old & b);
+                    edges += valid;
                 }
-                unsigned mask[4], total = 0;
-#pragma unroll
-                for (int k = 0; k < 4; k++) {
-                    mask[k] = __ballot_sync(kFull, mine[k]);
-                    total += __popc(mask[k]);
+                lanes_append(p, mine, v, u, len_next, out_head, out_tail, next_level, &s_err, lane, claimed);
+            }
+            // Vertices read through the CSR, four edges a step.
+            if (__any_sync(kFull, csr)) {
+                uint32_t s = 0, deg = 0;
+                if (csr) {
+                    s = __ldg(p.row_start + u);
+                    deg = __ldg(p.row_start + u + 1) - s;
                 }
-                if (total == 0) continue;  // warp uniform
-                unsigned at = 0;
-                if (lane == 0) at = atomicAdd(len_next, total);
-                at = __shfl_sync(kFull, at, 0);
+                edges += deg;
+                const unsigned max_deg = __reduce_max_sync(kFull, deg);
+                for (unsigned j = 0; j < max_deg; j += 4) {
+                    uint32_t v[4];
+                    bool mine[4];
 #pragma unroll
-                for (int k = 0; k < 4; k++) {
-                    if (mine[k]) {
-                        // Each vertex is claimed once, so a level appends
-                        // fewer than qcap = nnodes entries.
-                        const unsigned slot = at + __popc(mask[k] & lanemask_lt());
-                        if (slot < kLaneQueueHead)
-                            out_head[slot] = v[k];
-                        else if (slot < p.qcap)
-                            out_tail[slot] = v[k];
-                        else
-                            atomicCAS(&s_err, 0u, (unsigned)GFT_ERR_OVERFLOW);
-                        p.out[v[k]] = next_level;
-                        if (p.parent) p.parent[v[k]] = u;
-                        if (slots) prefetch_l1(slots + v[k]);
-                        claimed++;
+                    for (int k = 0; k < 4; k++) {
+                        v[k] = j + k < deg ? __ldg(p.edge_dst + s + j + k) : 0u;
+                        mine[k] = false;
+                        if (j + k < deg) {
+                            const uint32_t b = 1u << (v[k] & 31);
+                            if (v[k] < n)
+                                mine[k] = !(atomicOr(bits + (v[k] >> 5), b) & b);
+                            else
+                                atomicCAS(&s_err, 0u, (unsigned)GFT_ERR_FORMAT);
+                        }
                     }
-                    at += __popc(mask[k]);
+                    lanes_append(p, mine, v, u, len_next, out_head, out_tail, next_level, &s_err, lane, claimed);
                 }
             }
         }
@@ -281,10 +307,10 @@ __global__ void __launch_bounds__(BLOCK, 1) bfs_cta_lanes(TravParams p)
 __host__ __forceinline__ int lanes_block_for(uint32_t nnodes)
 {
     if (GFT_LANES_BLOCK) return GFT_LANES_BLOCK;
-    // Measured per query: the 256^2 grid (frontiers <= 256) runs in
-    // 0.60 / 0.62 / 0.69 ms at 256 / 512 / 1024 threads, the 362^2 road
-    // graph (random source, frontiers of 700 and more) in 0.75 / 0.50 /
-    // 0.42 ms.  Graphs here have at most kCtaLocalBitsNodes vertices.
+    // Idle warps still pay for every level's loop top and barrier: the
+    // 256^2 grid (frontiers <= 256) is fastest at 256 threads, the 362^2
+    // road graph (random sources, frontiers of 700 and more) at 1024.
+    // Graphs here have at most kCtaLocalBitsNodes vertices.
     return nnodes <= (1u << 16) ? 256 : 1024;
 }
 __host__ inline const void *lanes_kernel_for(int block)

@@ -102,7 +102,7 @@ def test_one_cta_bfs_either_side_of_the_shared_bitmap_limit(gft, orc, engine, si
 
 def test_one_cta_bfs_frontier_beyond_the_shared_queue_head(gft, orc, engine):
     """Small uniform-degree graphs run a thread per frontier vertex on one
-    CTA, with the first 16,384 entries of each frontier queue in shared
+    CTA, with the first 8,192 entries of each frontier queue in shared
     memory and the rest in global memory.  A random graph of 120,000
     vertices and degree <= 32 has levels of tens of thousands of vertices,
     so both parts of the queue carry vertices; levels and parents stay
@@ -131,6 +131,62 @@ def test_one_cta_bfs_frontier_beyond_the_shared_queue_head(gft, orc, engine):
             assert orc.check_tree(rs, dst, None, src, got, par) == 0
             assert r["grid_blocks"] == 1
             assert r["vertices_reached"] == int(reached.sum()) - 1  # the source is not counted
+
+
+def _wrap(gft, rs, dst):
+    """A device graph over caller-owned device arrays (no copy, no BFS slots)."""
+    import ctypes as C
+
+    import torch
+
+    d_rs = torch.from_numpy(rs.astype(np.int32)).cuda()
+    d_dst = torch.from_numpy(dst.astype(np.int32)).cuda()
+    h = C.c_void_p()
+    assert gft.load().gft_graph_wrap(0, len(rs) - 1, len(dst), C.c_void_p(d_rs.data_ptr()),
+                                     C.c_void_p(d_dst.data_ptr()), None, C.byref(h)) == 0
+    return gft.DeviceGraph(h, 0), (d_rs, d_dst)
+
+
+def test_one_cta_bfs_on_a_wrapped_graph(gft, orc, engine):
+    """A wrapped graph has no per-vertex slots, so the one-CTA kernel reads
+    every vertex through the CSR: a grid (degree <= 4) and a random graph
+    of degree <= 12 give the oracle's levels and valid parent trees."""
+    rng = np.random.default_rng(4)
+    grid = gft.CSRGraph.grid(90, 110, 0, 1)
+    n = 20_000
+    u = rng.integers(0, n, 50_000)
+    v = rng.integers(0, n, 50_000)
+    key = np.unique(np.concatenate([u * n + v, v * n + u]))
+    key = key[key // n != key % n]
+    src_of, dst = key // n, (key % n).astype(np.uint32)
+    deg = np.bincount(src_of, minlength=n)
+    first = np.concatenate([[0], np.cumsum(deg)[:-1]])
+    keep = np.arange(len(key)) - first[src_of] < 12  # at most 12 edges a vertex
+    src_of, dst = src_of[keep], dst[keep]
+    rs = np.zeros(n + 1, dtype=np.uint32)
+    np.cumsum(np.bincount(src_of, minlength=n), out=rs[1:])
+    for g_rs, g_dst in ((grid.row_start, grid.edge_dst), (rs, dst)):
+        dg, keep_alive = _wrap(gft, g_rs, g_dst)
+        for src in (0, len(g_rs) // 2):
+            want = orc.bfs(g_rs, g_dst, src)
+            got, par, r = _run_bfs(gft, engine, dg, src)
+            np.testing.assert_array_equal(got, want)
+            assert orc.check_tree(g_rs, g_dst, None, src, got, par) == 0
+            assert r["grid_blocks"] == 1
+        dg.free()
+
+
+def test_one_cta_bfs_reports_a_destination_outside_the_graph(gft, engine):
+    """An edge leaving the graph (only possible in wrapped, caller-owned
+    arrays) ends the one-CTA BFS with GFT_ERR_FORMAT, not a stray write."""
+    g = gft.CSRGraph.grid(40, 40, 0, 1)
+    dst = g.edge_dst.copy()
+    dst[len(dst) // 2] = g.nnodes + 5
+    dg, keep_alive = _wrap(gft, g.row_start, dst)
+    with pytest.raises(gft.GftError) as ei:
+        engine.bfs(dg, 0)
+    assert ei.value.status_name == "GFT_ERR_FORMAT"
+    dg.free()
 
 
 def test_road_sssp(gft, orc, engine):
