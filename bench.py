@@ -100,10 +100,13 @@ def tuned_for(gft, name: str, spec: dict):
     delta = spec.get("delta")
     if not t:
         return None, delta, None
-    tune = gft.Tune(block_threads=t["block_threads"], blocks_per_sm=t["blocks_per_sm"], hub_degree=t["hub_degree"])
+    keys = ("block_threads", "blocks_per_sm", "hub_degree", "queue_tile", "warp_degree")
+    if spec["app"] == "sssp":
+        keys += ("fuse_budget",)
+    tune = gft.Tune(**{k: t[k] for k in keys if k in t})
     if spec["app"] == "sssp" and "delta" in t:
         delta = t["delta"]
-    return tune, delta, {k: t[k] for k in ("block_threads", "blocks_per_sm", "hub_degree") if k in t}
+    return tune, delta, {k: t[k] for k in keys if k in t}
 L2_BYTES = 126 * 2**20
 
 

@@ -78,6 +78,8 @@ class Tuning(C.Structure):
         ("direction", C.c_uint32),
         ("cta_small", C.c_uint32),
         ("fuse_budget", C.c_uint32),
+        ("queue_tile", C.c_uint32),
+        ("warp_degree", C.c_uint32),
     ]
 
 

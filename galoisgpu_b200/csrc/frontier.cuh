@@ -26,6 +26,10 @@ __device__ __forceinline__ uint4 ld_stream4(const uint32_t *p) { return __ldcs(r
 // ---------------------------------------------------------------------------
 // Parameters
 // ---------------------------------------------------------------------------
+// Frontier vertices of at least this many edges are expanded by a whole
+// warp, smaller ones flattened across the warp (gft_tuning.warp_degree).
+constexpr uint32_t kDefaultWarpDegree = 32;
+
 struct TravParams {
     const uint32_t *__restrict__ row_start;
     const uint32_t *__restrict__ edge_dst;
@@ -54,6 +58,7 @@ struct TravParams {
     int uniform;  // every out-degree <= kUniformDegree: static chunks
     uint32_t cta_small;  // SSSP on the grid: iterations of at most this many vertices run on one CTA (0 = never)
     uint32_t fuse;       // SSSP: near vertices a warp may expand itself in the iteration that found them (0 = none)
+    uint32_t warp_degree = kDefaultWarpDegree;  // a vertex of at least this many edges is expanded by a whole warp
 };
 
 // ---------------------------------------------------------------------------
@@ -400,9 +405,10 @@ __device__ __forceinline__ void flatten_edges(Vis &vis, uint32_t start, uint32_t
     }
 }
 
-// Expands one vertex per lane (`has` false on idle lanes): degree >= 32 by
-// the whole warp, smaller lists flattened across it; vertices of degree >=
-// hub_degree go to the hub list for the grid-wide hub phase.
+// Expands one vertex per lane (`has` false on idle lanes): degree >=
+// p.warp_degree by the whole warp, smaller lists flattened across it;
+// vertices of degree >= hub_degree go to the hub list for the grid-wide hub
+// phase.
 template <class Vis, class Own>
 __device__ __forceinline__ void expand_lanes(Vis &vis, const TravParams &p, bool has, uint32_t u,
                                              unsigned long long *hub_ctr, unsigned lane)
@@ -430,14 +436,14 @@ __device__ __forceinline__ void expand_lanes(Vis &vis, const TravParams &p, bool
         else raise_error(&p.ctl->error, &p.ctl->error_where, GFT_ERR_OVERFLOW, h);
         deg = 0;
     }
-    unsigned m = __ballot_sync(kFull, deg >= 32);
+    unsigned m = __ballot_sync(kFull, deg >= p.warp_degree);
     while (m) {
         const int l = __ffs(m) - 1;
         m &= m - 1;
         const uint32_t s = __shfl_sync(kFull, start, l), d = __shfl_sync(kFull, deg, l);
         warp_range(vis, s, d, vis.shfl(o, l), lane);
     }
-    if (deg >= 32) deg = 0;
+    if (deg >= p.warp_degree) deg = 0;
     flatten_edges<Vis::kBatch>(vis, start, deg, o, lane);
 }
 

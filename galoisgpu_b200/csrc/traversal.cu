@@ -36,33 +36,36 @@ constexpr int kCtaBlock = 1024;  // threads of the single-CTA kernels
 // ---------------------------------------------------------------------------
 // Single-query kernels: the whole cooperative grid is one group.
 // ---------------------------------------------------------------------------
-// Push buffers of the grid-wide BFS kernel: 256 entries per warp (one
-// buffer per warp, at most 32 KB per CTA), as the grid-wide SSSP kernel.
+// Push buffers of the grid-wide kernels (the queue tile, QB entries per
+// warp) are a template parameter: 64, 128 or 256, picked per launch
+// (gft_tuning.queue_tile).  BFS defaults to 256 (one buffer per warp, at
+// most 32 KB per CTA), as the grid-wide SSSP kernel.
 constexpr unsigned kBfsGridQueueBuf = 256;
 
-template <int BLOCK>
+template <int BLOCK, unsigned QB>
 __global__ void __launch_bounds__(BLOCK, 2048 / BLOCK) bfs_persistent(TravParams p)
 {
-    __shared__ uint32_t s_buf[BLOCK / 32][kBfsGridQueueBuf];
+    __shared__ uint32_t s_buf[BLOCK / 32][QB];
     if ((int)blockIdx.x == p.skip_block) return;  // test hook: this CTA never arrives
     TraversalCtl *ctl = p.ctl;
     const unsigned tid = blockIdx.x * BLOCK + threadIdx.x, nthreads = gridDim.x * BLOCK;
     GridMode m{{&ctl->barrier.v, u32_of(ctl->release), &ctl->error, &ctl->error_where, gridDim.x, 0, p.timeout_ns},
                ctl, tid, nthreads, tid / 32, nthreads / 32};
-    bfs_body<GridMode, false, kBfsGridQueueBuf>(p, m, s_buf[threadIdx.x >> 5]);
+    bfs_body<GridMode, false, QB>(p, m, s_buf[threadIdx.x >> 5]);
 }
 
-// Push buffers of the grid-wide SSSP kernel: 256 entries per warp up to 512
-// threads per CTA (32 KB), halving the reservations on the piles' length
-// counters (road 4096^2: 3.74 -> 3.60 ms; 64 entries: 4.80 ms); 1024-thread
-// CTAs keep 128, the most that fits in 48 KB of static shared memory.
+// Default push buffers of the grid-wide SSSP kernel: 256 entries per warp up
+// to 512 threads per CTA (32 KB), halving the reservations on the piles'
+// length counters (road 4096^2: 3.74 -> 3.60 ms; 64 entries: 4.80 ms);
+// 1024-thread CTAs keep 128, the most that fits in 48 KB of static shared
+// memory (near and far buffers).
 template <int BLOCK>
 constexpr unsigned kSsspGridQueueBuf = BLOCK <= 512 ? 256 : kQueueBuf;
 
-template <int BLOCK>
+template <int BLOCK, unsigned QB>
 __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) sssp_persistent(TravParams p)
 {
-    constexpr unsigned QB = kSsspGridQueueBuf<BLOCK>;
+    static_assert(2 * (BLOCK / 32) * QB * 4 <= 48 * 1024, "near and far buffers exceed static shared memory");
     __shared__ uint32_t s_near[BLOCK / 32][QB];
     __shared__ uint32_t s_far[BLOCK / 32][QB];
     if ((int)blockIdx.x == p.skip_block) return;
@@ -416,22 +419,51 @@ constexpr uint32_t kDefaultFuse = 256;
 constexpr uint32_t kCtaMaxNodes = 1u << 17;
 constexpr uint32_t kCtaMaxEdges = 1u << 19;
 
-const void *bfs_kernel_for(int block)
+template <int BLOCK>
+const void *bfs_kernel_tile(uint32_t tile)
 {
-    switch (block) {
-    case 256: return (const void *)dev::bfs_persistent<256>;
-    case 512: return (const void *)dev::bfs_persistent<512>;
-    case 1024: return (const void *)dev::bfs_persistent<1024>;
+    switch (tile) {
+    case 64: return (const void *)dev::bfs_persistent<BLOCK, 64>;
+    case 128: return (const void *)dev::bfs_persistent<BLOCK, 128>;
+    case 256: return (const void *)dev::bfs_persistent<BLOCK, 256>;
     }
     return nullptr;
 }
 
-const void *sssp_kernel_for(int block)
+// Grid-wide BFS kernel for a CTA size and queue tile (0: the default tile);
+// NULL for a combination that is not built.
+const void *bfs_kernel_for(int block, uint32_t tile)
+{
+    if (!tile) tile = dev::kBfsGridQueueBuf;
+    switch (block) {
+    case 256: return bfs_kernel_tile<256>(tile);
+    case 512: return bfs_kernel_tile<512>(tile);
+    case 1024: return bfs_kernel_tile<1024>(tile);
+    }
+    return nullptr;
+}
+
+template <int BLOCK>
+const void *sssp_kernel_tile(uint32_t tile)
+{
+    switch (tile) {
+    case 64: return (const void *)dev::sssp_persistent<BLOCK, 64>;
+    case 128: return (const void *)dev::sssp_persistent<BLOCK, 128>;
+    case 256:
+        if constexpr (BLOCK <= 512) return (const void *)dev::sssp_persistent<BLOCK, 256>;
+        break;
+    }
+    return nullptr;
+}
+
+// Grid-wide SSSP kernel for a CTA size and queue tile (0: the default tile,
+// dev::kSsspGridQueueBuf); 1024-thread CTAs take tiles of at most 128.
+const void *sssp_kernel_for(int block, uint32_t tile)
 {
     switch (block) {
-    case 256: return (const void *)dev::sssp_persistent<256>;
-    case 512: return (const void *)dev::sssp_persistent<512>;
-    case 1024: return (const void *)dev::sssp_persistent<1024>;
+    case 256: return sssp_kernel_tile<256>(tile ? tile : dev::kSsspGridQueueBuf<256>);
+    case 512: return sssp_kernel_tile<512>(tile ? tile : dev::kSsspGridQueueBuf<512>);
+    case 1024: return sssp_kernel_tile<1024>(tile ? tile : dev::kSsspGridQueueBuf<1024>);
     }
     return nullptr;
 }
@@ -443,12 +475,14 @@ struct Tune {
     uint32_t direction;
     uint32_t cta_small;
     uint32_t fuse;
+    uint32_t tile;         // push-buffer entries per warp of the grid kernels (0 = default)
+    uint32_t warp_degree;  // degree from which a warp expands a vertex by itself
 };
 
 Tune resolve_tuning(const gft_tuning *t, bool is_sssp)
 {
     Tune r{is_sssp ? kDefaultBlockSssp : kDefaultBlockBfs, kDefaultBlocksPerSm, kDefaultHubDegree, kDefaultTimeoutMs,
-           -1, 0, 0, 0, 0};
+           -1, 0, 0, 0, 0, 0, dev::kDefaultWarpDegree};
     if (t) {
         if (t->block_threads) r.block = t->block_threads;
         if (t->blocks_per_sm) r.bps = t->blocks_per_sm;
@@ -459,6 +493,8 @@ Tune resolve_tuning(const gft_tuning *t, bool is_sssp)
         r.direction = t->direction;
         r.cta_small = t->cta_small;
         r.fuse = t->fuse_budget;
+        r.tile = t->queue_tile;
+        if (t->warp_degree) r.warp_degree = t->warp_degree;
     }
     return r;
 }
@@ -507,8 +543,12 @@ gft_status run_traversal(bool is_sssp, gft_engine *e, const gft_graph *g, uint32
     if (is_sssp && G.edge_data && !G.edge_dw && !G.wrapped)
         GFT_TRY(ensure_edge_pairs(const_cast<gft_graph *>(g), stream));
     Tune t = resolve_tuning(tune, is_sssp);
-    const void *kern = is_sssp ? sssp_kernel_for(t.block) : bfs_kernel_for(t.block);
-    if (!kern) return fail(GFT_ERR_INVALID_ARG, "%s: block_threads must be 256, 512 or 1024", what);
+    const void *kern = is_sssp ? sssp_kernel_for(t.block, t.tile) : bfs_kernel_for(t.block, t.tile);
+    if (!kern)
+        return fail(GFT_ERR_INVALID_ARG,
+                    "%s: block_threads must be 256, 512 or 1024 and queue_tile 0, 64, 128 or 256 "
+                    "(SSSP at 1024 threads: at most 128)",
+                    what);
     if (t.hub < 32) t.hub = 32;
     DeviceScope device_scope(e->device);
     GFT_CUDA_TRY(device_scope.err);
@@ -592,6 +632,7 @@ gft_status run_traversal(bool is_sssp, gft_engine *e, const gft_graph *g, uint32
     }
     p.hub_cap = hub_cap;
     p.hub_degree = t.hub;
+    p.warp_degree = t.warp_degree;
     p.qcap = qcap;
     p.delta = (uint32_t)delta;
     p.ctl = reinterpret_cast<TraversalCtl *>(e->ctl.ptr);
@@ -846,7 +887,7 @@ extern "C" gft_status gft_bfs_noalloc(const gft_graph *g, uint32_t src, int32_t 
     char *base = nullptr;
     GFT_TRY(noalloc_scratch(G.device, &base));
 
-    const void *kern = (const void *)dev::bfs_persistent<kNoAllocBlock>;
+    const void *kern = (const void *)dev::bfs_persistent<kNoAllocBlock, dev::kBfsGridQueueBuf>;
     int sms = 0, occ = 0;
     GFT_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, G.device));
     GFT_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kNoAllocBlock, 0));

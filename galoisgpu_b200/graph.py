@@ -292,11 +292,13 @@ class Tune:
     direction: int = 0  # BFS: 0 = direction-optimising on graphs marked symmetric, 1 = top-down only
     cta_small: int = 0  # SSSP on the grid: iterations up to this many vertices on one CTA (0 = default, 2**32-1 = never)
     fuse_budget: int = 0  # SSSP: near vertices a warp expands in the iteration that found them (0 = default, 2**32-1 = never)
+    queue_tile: int = 0  # grid kernels: push-buffer entries per warp, 64 / 128 / 256 (0 = default)
+    warp_degree: int = 0  # vertices of at least this many edges are expanded by a whole warp (0 = 32)
 
     def c(self) -> Tuning:
         return Tuning(self.block_threads, self.blocks_per_sm, self.hub_degree, self.timeout_ms, self.test_skip_block,
                       self.max_blocks, self.group_blocks, self.group_min_nodes, self.direction, self.cta_small,
-                      self.fuse_budget)
+                      self.fuse_budget, self.queue_tile, self.warp_degree)
 
 
 class Engine:

@@ -112,6 +112,13 @@ typedef struct gft_tuning {
                                  never on skewed ones; UINT32_MAX = never;
                                  near piles above 524288 vertices are never
                                  fused)                                       */
+    uint32_t queue_tile;      /* grid-wide kernels: push-buffer entries per warp,
+                                 64, 128 or 256 (0 = engine default: 256, and
+                                 128 for SSSP at 1024 threads, whose two
+                                 buffers then take at most 128)               */
+    uint32_t warp_degree;     /* frontier vertices of at least this many edges
+                                 are expanded by a whole warp, smaller ones
+                                 flattened across the warp (0 = 32)           */
 } gft_tuning;
 
 /* ---------------------------------------------------------------------------

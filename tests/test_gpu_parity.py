@@ -15,8 +15,10 @@ TUNES = [
     dict(block_threads=1024, blocks_per_sm=1, max_blocks=1 << 30),
     dict(hub_degree=32, max_blocks=1 << 30),  # every vertex of degree >= 32 goes through the grid-wide hub phase
     dict(max_blocks=1, hub_degree=32),  # always one CTA
+    dict(queue_tile=64, warp_degree=8, max_blocks=1 << 30),  # small push buffers, warps from degree 8
+    dict(block_threads=512, queue_tile=256, warp_degree=128, max_blocks=1 << 30),  # edge lists < 128 flattened
 ]
-TUNE_IDS = ["auto", "grid256x4", "grid1024x1", "grid-hub32", "one-cta"]
+TUNE_IDS = ["auto", "grid256x4", "grid1024x1", "grid-hub32", "one-cta", "tile64-warp8", "tile256-warp128"]
 
 
 def _sources(n):
@@ -324,6 +326,22 @@ def test_barrier_timeout_is_reported_and_engine_recovers(gft, orc, engine):
     assert ei.value.status_name == "GFT_ERR_TIMEOUT"
     r = engine.bfs(dg, 0)
     np.testing.assert_array_equal(r["out"].cpu().numpy(), orc.bfs(g.row_start, g.edge_dst, 0))
+
+
+def test_queue_tile_must_be_built(gft, engine):
+    """Queue tiles are 64, 128 or 256 entries a warp; SSSP at 1024 threads
+    takes at most 128 (its near and far buffers share 48 KB of static
+    shared memory).  Anything else is GFT_ERR_INVALID_ARG, not a launch."""
+    g = gft.CSRGraph.rmat(12, 8, seed=3, max_weight=255)
+    dg = g.copy_to_gpu()
+    for app, tune in (("bfs", dict(queue_tile=96)), ("sssp", dict(block_threads=1024, queue_tile=256)),
+                      ("sssp", dict(queue_tile=512))):
+        t = gft.Tune(max_blocks=1 << 30, **tune)
+        with pytest.raises(gft.GftError) as ei:
+            engine.sssp(dg, 0, tune=t) if app == "sssp" else engine.bfs(dg, 0, tune=t)
+        assert ei.value.status_name == "GFT_ERR_INVALID_ARG"
+    ok = engine.sssp(dg, 0, tune=gft.Tune(block_threads=1024, queue_tile=128, max_blocks=1 << 30))
+    assert ok["out"].cpu().numpy()[0] == 0
 
 
 def test_invalid_arguments(gft, engine):
