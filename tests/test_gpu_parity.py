@@ -135,6 +135,45 @@ def test_one_cta_bfs_frontier_beyond_the_shared_queue_head(gft, orc, engine):
             assert r["vertices_reached"] == int(reached.sum()) - 1  # the source is not counted
 
 
+def test_one_cta_bfs_on_graphs_with_odd_cycles(gft, orc, engine):
+    """Random graphs of degree <= 4 (the one-CTA kernel's per-vertex slot
+    path; 131,000 vertices take the 1024-thread CTA) and <= 9 (some
+    vertices through the CSR), full of odd cycles, so that a level's
+    vertices also claim one another's neighbours: levels, the level count
+    and the reached count equal the oracle's, and parent trees are valid,
+    with and without the parent output."""
+    import torch
+
+    rng = np.random.default_rng(31)
+    for n, cap in ((30_000, 4), (50_000, 9), (131_000, 4)):
+        u = rng.integers(0, n, 3 * n)
+        v = rng.integers(0, n, 3 * n)
+        key = np.unique(np.concatenate([u * n + v, v * n + u]))
+        key = key[key // n != key % n]
+        src_of, dst = key // n, key % n
+        deg = np.bincount(src_of, minlength=n)
+        first = np.concatenate([[0], np.cumsum(deg)[:-1]])
+        rank = np.arange(len(key)) - first[src_of]
+        keep = rank < cap
+        pairs = set(zip(src_of[keep].tolist(), dst[keep].tolist()))
+        sym = np.array(sorted(p for p in pairs if (p[1], p[0]) in pairs), dtype=np.int64)
+        rs = np.zeros(n + 1, dtype=np.uint32)
+        np.cumsum(np.bincount(sym[:, 0], minlength=n), out=rs[1:])
+        g = gft.CSRGraph(rs, sym[:, 1].astype(np.uint32), None)
+        dg = g.copy_to_gpu()
+        for src in g.pick_sources(5, 3):
+            want = orc.bfs(g.row_start, g.edge_dst, src)
+            got, par, r = _run_bfs(gft, engine, dg, src)
+            np.testing.assert_array_equal(got, want)
+            assert orc.check_tree(g.row_start, g.edge_dst, None, src, got, par) == 0
+            assert r["grid_blocks"] == 1
+            reached = want != np.iinfo(np.int32).max
+            assert r["levels"] == int(want[reached].max()) + 1
+            assert r["vertices_reached"] == int(reached.sum()) - 1
+            out = torch.empty(dg.nnodes, dtype=torch.int32, device="cuda")
+            np.testing.assert_array_equal(engine.bfs(dg, src, out=out)["out"].cpu().numpy(), want)
+
+
 def _wrap(gft, rs, dst):
     """A device graph over caller-owned device arrays (no copy, no BFS slots)."""
     import ctypes as C
