@@ -926,8 +926,8 @@ def bench_msbfs(gft, dev: int, k: int = 256, reps: int = 3, max_levels: int = 16
     }
 
 
-def bench_serve(gft, dev: int, rates=(200, 1000, 3000, 10000, 50000),
-                p99_targets=(10.0, 20.0, 50.0, 100.0, 500.0), delta: int = 40000) -> dict:
+def bench_serve(gft, dev: int, rates=(200, 500, 1000, 3000, 10000, 50000),
+                p99_targets=(10.0, 20.0, 50.0, 100.0, 200.0, 500.0), delta: int = 40000) -> dict:
     """C5: Poisson BFS/SSSP requests with random non-isolated sources over
     resident graphs, at offered rates from 200 to 50,000 requests/s, against
     - the resident serving kernel (one persistent launch; requests through a

@@ -64,7 +64,8 @@
 namespace gft {
 
 constexpr unsigned kResMaxLanes = 64;  // one bit per lane in the idle mask
-constexpr unsigned long long kGatherNs = 3000000;  // longest wait of a large job for its minimum width
+constexpr unsigned long long kGatherNs = 3000000;       // a large job's gather with other claims held back
+constexpr unsigned long long kGatherLongNs = 12000000;  // its longest gather while it has under half its width
 constexpr unsigned kCmdRun = 1, kCmdExit = 2;
 
 struct alignas(128) ResLaneBox {
@@ -91,7 +92,8 @@ struct ResDev {
     unsigned long long last_busy;  // %globaltimer of the last claim or completion (0 at launch)
     unsigned head;                 // next ring index to claim (persists across launches)
     unsigned closing;              // set once: every lane leaves as soon as it is idle
-    unsigned pad[26];
+    unsigned gathering;            // leaders gathering lanes for a large job: idle lanes claim nothing meanwhile
+    unsigned pad[25];
     ResLaneBox box[kResMaxLanes];
     ResTeam team[kResMaxLanes];
 };
@@ -269,13 +271,26 @@ __device__ bool lead_team(const ResArgs &a, unsigned lane, unsigned long long h,
     unsigned long long got = 0;
     if (pick) got = atomicAnd(&S->idle, ~pick) & pick;
     // A large job that found too few idle lanes gathers more as other teams
-    // finish, for at most kGatherNs: on one or two lanes it would run several
-    // times longer than on its minimum.
+    // finish: on one or two lanes it would run 30-40 times longer than
+    // alone.  For up to kGatherNs idle lanes claim no new job meanwhile, so
+    // the lanes that other teams free come to it; after that it competes
+    // with new claims, and it keeps gathering only while it has fewer than
+    // half of its lanes, up to kGatherLongNs.  (Holding claims back for the
+    // whole gather cost a quarter of the saturated throughput.)
     const unsigned need = min(max(T.job.min_lanes, 1u), a.max_team_lanes);
     if ((unsigned)__popcll(got) + 1 < need) {
+        atomicAdd(&S->gathering, 1u);
+        bool holding = true;
         const unsigned long long tg = globaltimer_ns();
         unsigned sleep_ns = 64;
-        while ((unsigned)__popcll(got) + 1 < need && globaltimer_ns() - tg < kGatherNs) {
+        for (;;) {
+            const unsigned have = (unsigned)__popcll(got) + 1;
+            const unsigned long long waited = globaltimer_ns() - tg;
+            if (holding && (have >= need || waited >= kGatherNs)) {
+                atomicSub(&S->gathering, 1u);
+                holding = false;
+            }
+            if (have >= need || (!holding && (2 * have >= need || waited >= kGatherLongNs))) break;
             unsigned long long more = ld_relaxed_u64(&S->idle) & ~mine & ~got;
             unsigned long long take = 0;
             for (unsigned k = __popcll(got) + 1; k < need && more; k++) {
@@ -342,6 +357,13 @@ __device__ void lane_leader_idle(const ResArgs &a, unsigned lane, unsigned seen,
         if (!ld_relaxed_u32(&S->closing)) {
             const unsigned long long tail = ld_acquire_sys_u64(&a.H->tail);
             const unsigned head = ld_relaxed_u32(&S->head);
+            if (head < tail && ld_relaxed_u32(&S->gathering) != 0) {
+                // A leader gathers lanes for a large job: stay idle to be
+                // drafted (bounded: a gather lasts at most kGatherNs).
+                __nanosleep(sleep_ns);
+                sleep_ns = min(sleep_ns * 2, 256u);
+                continue;
+            }
             if (head < tail) {
                 const unsigned long long old = atomicAnd(&S->idle, ~mine);
                 if (!(old & mine)) {  // drafted meanwhile: the mailbox gets the command
@@ -557,13 +579,13 @@ namespace {
 // Launches the resident kernel (mu held).  All lanes start idle.
 gft_status launch_locked(ResidentServer *s)
 {
-    // idle = every lane, last_busy = 0, closing = 0; head persists.
+    // idle = every lane, last_busy = 0, closing = gathering = 0; head persists.
     static const unsigned long long zero = 0;
     const unsigned long long all = s->nlanes >= 64 ? ~0ull : ((1ull << s->nlanes) - 1);
     s->all_lanes = all;
     GFT_CUDA_TRY(cudaMemcpyAsync(&s->D->idle, &s->all_lanes, sizeof all, cudaMemcpyHostToDevice, s->stream));
     GFT_CUDA_TRY(cudaMemcpyAsync(&s->D->last_busy, &zero, sizeof zero, cudaMemcpyHostToDevice, s->stream));
-    GFT_CUDA_TRY(cudaMemsetAsync(&s->D->closing, 0, sizeof(unsigned), s->stream));
+    GFT_CUDA_TRY(cudaMemsetAsync(&s->D->closing, 0, 2 * sizeof(unsigned), s->stream));  // closing, gathering
     // Mailboxes and control blocks: nothing of an earlier launch is left in them.
     GFT_CUDA_TRY(cudaMemsetAsync(s->D->box, 0, sizeof(s->D->box), s->stream));
     GFT_CUDA_TRY(cudaMemsetAsync(s->D->team, 0, sizeof(s->D->team), s->stream));
