@@ -146,10 +146,11 @@ constexpr size_t kLaneSmemBytes = (kCtaLocalBitsNodes / 32 + 2 * (size_t)kLaneQu
 // One warp step's appends: claimed destinations v[k] (mine[k]) of frontier
 // vertex u go to the next frontier and get their level.  Each vertex is
 // claimed once, so a level appends fewer than qcap = nnodes entries.
+template <bool kParent>
 __device__ __forceinline__ void lanes_append(const TravParams &p, const bool (&mine)[4], const uint32_t (&v)[4],
                                              uint32_t u, unsigned *len_next, uint32_t *out_head,
                                              uint32_t *out_tail, int32_t level, unsigned *err, unsigned lane,
-                                             unsigned long long &claimed)
+                                             unsigned &claimed)
 {
     unsigned mask[4], total = 0;
 #pragma unroll
@@ -171,7 +172,7 @@ __device__ __forceinline__ void lanes_append(const TravParams &p, const bool (&m
             if (mine[k]) {
                 out_head[at + __popc(mask[k] & lt)] = v[k];
                 p.out[v[k]] = level;
-                if (p.parent) p.parent[v[k]] = u;
+                if (kParent) p.parent[v[k]] = u;
             }
             at += __popc(mask[k]);
         }
@@ -188,13 +189,13 @@ __device__ __forceinline__ void lanes_append(const TravParams &p, const bool (&m
             else
                 atomicCAS(err, 0u, (unsigned)GFT_ERR_OVERFLOW);
             p.out[v[k]] = level;
-            if (p.parent) p.parent[v[k]] = u;
+            if (kParent) p.parent[v[k]] = u;
         }
         at += __popc(mask[k]);
     }
 }
 
-template <int BLOCK>
+template <int BLOCK, bool kParent>
 __global__ void __launch_bounds__(BLOCK, 1) bfs_cta_lanes(TravParams p)
 {
     extern __shared__ __align__(16) uint32_t s_lane[];
@@ -206,7 +207,7 @@ __global__ void __launch_bounds__(BLOCK, 1) bfs_cta_lanes(TravParams p)
     const uint32_t n = p.nnodes, nwords = (n + 31) >> 5;
     for (uint32_t v = tid; v < n; v += BLOCK) {
         p.out[v] = v == p.src ? 0 : (int32_t)kInf;
-        if (p.parent) p.parent[v] = v == p.src ? p.src : GFT_NO_PARENT;
+        if (kParent) p.parent[v] = v == p.src ? p.src : GFT_NO_PARENT;
     }
     for (uint32_t w = tid; w < nwords; w += BLOCK) bits[w] = w == (p.src >> 5) ? 1u << (p.src & 31) : 0u;
     if (tid == 0) {
@@ -220,19 +221,23 @@ __global__ void __launch_bounds__(BLOCK, 1) bfs_cta_lanes(TravParams p)
 
     const uint4 *__restrict__ slots = p.bfs_slots;
     const uint4 none = make_uint4(kBfsSlotNone, kBfsSlotNone, kBfsSlotNone, kBfsSlotNone);
-    unsigned long long edges = 0, claimed = 0;
+    // Per-thread counts fit 32 bits: graphs here have at most 2^17 vertices
+    // of at most kUniformDegree edges.
+    unsigned edges = 0, claimed = 0;
     unsigned L = 0;
+    // Lengths are triple-buffered: s_len[c] is read by every thread at the
+    // top of a level, s_len[nx] collects the level's appends, and s_len[cl]
+    // (read at the top of the previous level, before its barrier) is
+    // cleared for the next level; the three rotate each level, as the two
+    // queues swap.
+    unsigned c = 0, nx = 1, cl = 2;
+    const uint32_t *in_head = head0, *in_tail = p.q[0];
+    uint32_t *out_head = head1, *out_tail = p.q[1];
     for (;;) {
-        // Lengths are triple-buffered: slot L % 3 is read by every thread
-        // here, slot (L + 1) % 3 collects this level's appends, and slot
-        // (L + 2) % 3 (read at the top of the previous level, before its
-        // barrier) is cleared for the next level.
-        const unsigned n_in = *(volatile unsigned *)&s_len[L % 3];
+        const unsigned n_in = *(volatile unsigned *)&s_len[c];
         if (n_in == 0) break;
-        if (tid == 0) s_len[(L + 2) % 3] = 0;
-        unsigned *len_next = &s_len[(L + 1) % 3];
-        const uint32_t *in_head = (L & 1) ? head1 : head0, *in_tail = sel2(p.q, L);
-        uint32_t *out_head = (L & 1) ? head0 : head1, *out_tail = sel2(p.q, L + 1);
+        if (tid == 0) s_len[cl] = 0;
+        unsigned *len_next = &s_len[nx];
         const int32_t next_level = (int32_t)L + 1;
         for (unsigned base = tid - lane; base < n_in; base += BLOCK) {  // warp-uniform trip count
             const unsigned i = base + lane;
@@ -260,7 +265,8 @@ __global__ void __launch_bounds__(BLOCK, 1) bfs_cta_lanes(TravParams p)
                     mine[k] = !(old & b);
                     edges += valid;
                 }
-                lanes_append(p, mine, v, u, len_next, out_head, out_tail, next_level, &s_err, lane, claimed);
+                lanes_append<kParent>(p, mine, v, u, len_next, out_head, out_tail, next_level, &s_err, lane,
+                                      claimed);
             }
             // Vertices read through the CSR, four edges a step.
             if (__any_sync(kFull, csr)) {
@@ -286,7 +292,8 @@ __global__ void __launch_bounds__(BLOCK, 1) bfs_cta_lanes(TravParams p)
                                 atomicCAS(&s_err, 0u, (unsigned)GFT_ERR_FORMAT);
                         }
                     }
-                    lanes_append(p, mine, v, u, len_next, out_head, out_tail, next_level, &s_err, lane, claimed);
+                    lanes_append<kParent>(p, mine, v, u, len_next, out_head, out_tail, next_level, &s_err, lane,
+                                          claimed);
                 }
             }
         }
@@ -294,6 +301,15 @@ __global__ void __launch_bounds__(BLOCK, 1) bfs_cta_lanes(TravParams p)
         const bool failed = __syncthreads_or(*(volatile unsigned *)&s_err != 0);
         L++;
         if (failed) break;
+        const unsigned c0 = c;
+        c = nx;
+        nx = cl;
+        cl = c0;
+        const uint32_t *ih = in_head, *it = in_tail;
+        in_head = out_head;
+        in_tail = out_tail;
+        out_head = const_cast<uint32_t *>(ih);
+        out_tail = const_cast<uint32_t *>(it);
     }
     warp_add_u64(&p.ctl->edges, edges, lane);
     warp_add_u64(&p.ctl->reached, claimed, lane);
@@ -316,15 +332,22 @@ __host__ __forceinline__ int lanes_block_for(uint32_t nnodes)
     // Graphs here have at most kCtaLocalBitsNodes vertices.
     return nnodes <= (1u << 16) ? 256 : 1024;
 }
+template <bool kParent>
 __host__ inline const void *lanes_kernel_for(int block)
 {
-    return block <= 256 ? (const void *)bfs_cta_lanes<256>
-                        : block <= 512 ? (const void *)bfs_cta_lanes<512> : (const void *)bfs_cta_lanes<1024>;
+    return block <= 256   ? (const void *)bfs_cta_lanes<256, kParent>
+           : block <= 512 ? (const void *)bfs_cta_lanes<512, kParent>
+                          : (const void *)bfs_cta_lanes<1024, kParent>;
+}
+__host__ inline const void *lanes_kernel_for(int block, bool parent)
+{
+    return parent ? lanes_kernel_for<true>(block) : lanes_kernel_for<false>(block);
 }
 __host__ inline bool is_lanes_kernel(const void *k)
 {
-    return k == (const void *)bfs_cta_lanes<256> || k == (const void *)bfs_cta_lanes<512> ||
-           k == (const void *)bfs_cta_lanes<1024>;
+    for (int b : {256, 512, 1024})
+        if (k == lanes_kernel_for<false>(b) || k == lanes_kernel_for<true>(b)) return true;
+    return false;
 }
 
 __global__ void __launch_bounds__(kCtaBlock, 1) sssp_single_cta(TravParams p)
@@ -572,7 +595,7 @@ gft_status run_traversal(bool is_sssp, gft_engine *e, const gft_graph *g, uint32
             // these graphs stay near the square root of the vertex count.
             const int lanes_block = dev::lanes_block_for(G.nnodes);
             shape.block_threads = lanes_block;
-            kern = dev::lanes_kernel_for(lanes_block);
+            kern = dev::lanes_kernel_for(lanes_block, d_parent != nullptr);
             dyn_smem = dev::kLaneSmemBytes;
             if (!G.wrapped) GFT_TRY(ensure_bfs_slots(const_cast<gft_graph *>(g), stream));
             GFT_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn_smem));
