@@ -297,10 +297,11 @@ __global__ void __launch_bounds__(BLOCK, 1) bfs_cta_lanes(TravParams p)
                 }
             }
         }
-        // Every thread gets the same answer, so all leave at the same level.
-        const bool failed = __syncthreads_or(*(volatile unsigned *)&s_err != 0);
+        // An error (a destination outside the graph, a queue overrun) skips
+        // the access it found and is reported after the traversal, so the
+        // level ends with a plain barrier.
+        __syncthreads();
         L++;
-        if (failed) break;
         const unsigned c0 = c;
         c = nx;
         nx = cl;
