@@ -405,16 +405,31 @@ def bench_workload(gft, name: str, steps: int, warmup: int, d, dev: int, headlin
 
 
 def cpu_baseline(orc, spec, host, src, reach, gpu_out=None) -> dict:
+    """The oracle's query on one host core.  A query of under 0.1 s is
+    repeated for about a second and its median taken, so that a
+    sub-millisecond baseline is not one noisy sample."""
+    def run():
+        if spec["app"] == "sssp":
+            return orc.sssp(host.row_start, host.edge_dst, host.edge_data, src)
+        return orc.bfs(host.row_start, host.edge_dst, src)
+
     t = time.perf_counter()
-    if spec["app"] == "sssp":
-        ref = orc.sssp(host.row_start, host.edge_dst, host.edge_data, src)
-    else:
-        ref = orc.bfs(host.row_start, host.edge_dst, src)
+    ref = run()
     dt = time.perf_counter() - t
+    times = [dt]
+    if dt < 0.1:
+        t_end = time.perf_counter() + 1.0
+        while time.perf_counter() < t_end and len(times) < 5000:
+            t = time.perf_counter()
+            run()
+            times.append(time.perf_counter() - t)
+        dt = statistics.median(times[1:])
     e_r = reach[src][1]
-    res = {"value": e_r / dt / 1e9, "unit": "GTEPS", "cores": 1, "kind": "port",
-           "sample": f"one full {spec['app'].upper()} query from source {src} "
-                     f"({'binary-heap Dijkstra' if spec['app'] == 'sssp' else 'FIFO BFS'}, {dt:.1f} s)"}
+    algo = "binary-heap Dijkstra" if spec["app"] == "sssp" else "FIFO BFS"
+    sample = (f"one full {spec['app'].upper()} query from source {src} ({algo}, {dt:.1f} s)" if len(times) == 1 else
+              f"the median of {len(times) - 1} full {spec['app'].upper()} queries from source {src} ({algo}, "
+              f"{dt * 1e3:.3f} ms each; min {min(times[1:]) * 1e3:.3f} ms)")
+    res = {"value": e_r / dt / 1e9, "unit": "GTEPS", "cores": 1, "kind": "port", "sample": sample}
     parity = None
     if gpu_out is not None:
         parity = "bit-exact" if np.array_equal(ref, gpu_out) else "MISMATCH"
