@@ -5,8 +5,12 @@ tuning/bfstuner.py, tuning/sssptuner.py), which rebuilt the binary per block
 size and scraped its output.  Here every tunable is a launch-time parameter,
 so a candidate costs only a few queries on a resident graph:
 
-  block_threads   CTA size of the persistent kernel (256 / 512 / 1024)
-  blocks_per_sm   persistent CTAs per SM (capped by occupancy)
+  block_threads   CTA size of the persistent kernel (256 / 512 / 1024) and
+  blocks_per_sm   persistent CTAs per SM (capped by occupancy), swept as one
+                  axis of pairs: the best pair can be worse than its
+                  neighbours on both single axes (BFS on RMAT-24: 512 x 4
+                  0.70 ms, 1024 x 2 0.74 ms, 512 x 2 0.96 ms, 1024 x 4 capped
+                  to 1024 x 2), which a one-axis step never crosses
   hub_degree      degree at which a frontier vertex is split across the grid
   queue_tile      push-buffer entries per warp (64 / 128 / 256; kernels are
                   built for each, so the tile is picked per launch; the
@@ -44,6 +48,8 @@ from .graph import DEFAULT_DELTA, DeviceGraph, Engine, Tune
 
 BLOCKS = (256, 512, 1024)
 BLOCKS_PER_SM = (1, 2, 3, 4)
+SHAPE = ("block_threads", "blocks_per_sm")  # swept together
+SHAPES = tuple((b, k) for b in BLOCKS for k in BLOCKS_PER_SM)
 HUB_DEGREES = (256, 1024, 4096, 16384, 65536)
 QUEUE_TILES = (64, 128, 256)
 WARP_DEGREES = (8, 16, 32, 64, 128)
@@ -97,6 +103,26 @@ def _time(engine: Engine, graph: DeviceGraph, app: str, sources, cand: Tuned, re
     return statistics.median(ms)
 
 
+def _fields(axes: dict) -> list:
+    """Tuned fields the axes cover (an axis is a field name or a tuple of them)."""
+    out = []
+    for a in axes:
+        out.extend(a if isinstance(a, tuple) else (a,))
+    return out
+
+
+def _get(t: Tuned, axis):
+    return tuple(getattr(t, f) for f in axis) if isinstance(axis, tuple) else getattr(t, axis)
+
+
+def _set(t: Tuned, axis, value) -> None:
+    if isinstance(axis, tuple):
+        for f, v in zip(axis, value):
+            setattr(t, f, v)
+    else:
+        setattr(t, axis, value)
+
+
 def autotune(engine: Engine, graph: DeviceGraph, app: str, sources, reps: int = 3, rounds: int = 2,
              axes: dict | None = None, log=None, uniform: bool = False, out=None) -> Tuned:
     """Coordinate-descent search from the engine defaults (`uniform`: the
@@ -108,33 +134,35 @@ def autotune(engine: Engine, graph: DeviceGraph, app: str, sources, reps: int = 
 
         out = torch.empty(graph.nnodes, dtype=torch.int32, device=f"cuda:{graph.device}")
     axes = dict(axes or {})
-    axes.setdefault("block_threads", BLOCKS)
-    axes.setdefault("blocks_per_sm", BLOCKS_PER_SM)
+    if "block_threads" not in axes and "blocks_per_sm" not in axes:
+        axes.setdefault(SHAPE, SHAPES)
     axes.setdefault("hub_degree", HUB_DEGREES)
     axes.setdefault("queue_tile", QUEUE_TILES)
     axes.setdefault("warp_degree", WARP_DEGREES)
     if app == "sssp":
         axes.setdefault("delta", DELTAS)
         axes.setdefault("fuse_budget", FUSE_BUDGETS)
+    fields = _fields(axes)
     best = start_point(app, uniform)
     best.ms = _time(engine, graph, app, sources, best, reps, out)
-    best.trials.append({**{k: getattr(best, k) for k in axes}, "ms": best.ms})
+    best.trials.append({**{k: getattr(best, k) for k in fields}, "ms": best.ms})
     for _ in range(rounds):
         improved = False
         for axis, values in axes.items():
             for v in values:
-                if getattr(best, axis) == v:
+                if _get(best, axis) == v:
                     continue
                 cand = Tuned(**{**asdict(best), "trials": []})
-                setattr(cand, axis, v)
+                _set(cand, axis, v)
                 if app == "sssp" and cand.block_threads == 1024:
                     cand.queue_tile = min(cand.queue_tile, 128)  # the largest SSSP tile built at 1024 threads
                 t = _time(engine, graph, app, sources, cand, reps, out)
-                best.trials.append({**{k: getattr(cand, k) for k in axes}, "ms": t})
+                best.trials.append({**{k: getattr(cand, k) for k in fields}, "ms": t})
                 if log:
-                    log(f"{axis}={v}: {t:.3f} ms (best {best.ms:.3f})")
+                    name = "x".join(axis) if isinstance(axis, tuple) else axis
+                    log(f"{name}={v}: {t:.3f} ms (best {best.ms:.3f})")
                 if t < best.ms * 0.99:
-                    for k in axes:
+                    for k in fields:
                         setattr(best, k, getattr(cand, k))
                     best.ms = t
                     improved = True

@@ -43,7 +43,15 @@ constexpr int kCtaBlock = 1024;  // threads of the single-CTA kernels
 constexpr unsigned kBfsGridQueueBuf = 256;
 
 template <int BLOCK, unsigned QB>
-__global__ void __launch_bounds__(BLOCK, 2048 / BLOCK) bfs_persistent(TravParams p)
+// Resident threads per SM the grid BFS kernel's register budget is set for:
+// 2048 (32 registers a thread, 42 bytes spilled).  A 64-register build
+// (1024, no spills) was slower on RMAT-24 BFS: best 0.89 ms against 0.70 ms
+// (512 x 4) and 0.74 ms (1024 x 2); more warps in flight hide more of the
+// traversal's memory latency than the spills cost.
+#ifndef GFT_BFS_THREADS_PER_SM
+#define GFT_BFS_THREADS_PER_SM 2048
+#endif
+__global__ void __launch_bounds__(BLOCK, GFT_BFS_THREADS_PER_SM / BLOCK) bfs_persistent(TravParams p)
 {
     __shared__ uint32_t s_buf[BLOCK / 32][QB];
     if ((int)blockIdx.x == p.skip_block) return;  // test hook: this CTA never arrives

@@ -64,6 +64,24 @@ def test_search_reaches_the_optimum_and_skips_unbuilt_tiles(gft):
     assert (bfs.block_threads, bfs.queue_tile, bfs.warp_degree) == (1024, 128, 64)
 
 
+def test_cta_size_and_count_are_swept_together(gft):
+    """An optimum that no single-axis step reaches: the start (512, 2) costs
+    3, one step on the CTA size reaches (1024, 2) at 2, and from there no
+    single step on either axis reaches (512, 4) at 1."""
+    from galoisgpu_b200 import autotune as at
+
+    class Ridge(_FakeEngine):
+        def _ms(self, values):
+            shape = {(512, 4): 1.0, (1024, 2): 2.0, (512, 2): 3.0}.get(
+                (values["block_threads"], values["blocks_per_sm"]), 5.0)
+            return shape + 0.01 * sum(abs(self.ORDER[k].index(v) - self.ORDER[k].index(self.OPT[k]))
+                                      for k, v in values.items() if k not in ("block_threads", "blocks_per_sm"))
+
+    best = at.autotune(Ridge(gft), _FakeGraph(), "bfs", [0], reps=1, rounds=4, out=object())
+    assert (best.block_threads, best.blocks_per_sm) == (512, 4)
+    assert {"block_threads", "blocks_per_sm"} <= set(best.trials[0])
+
+
 def test_start_point_is_the_engine_default():
     from galoisgpu_b200 import autotune as at
 
